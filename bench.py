@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark of the RCWA solve path on B200.
+
+Workload (one "step"): the 3-layer spectral sweep -- period 400x400 nm, line
+grating (120 nm) / hole array r=100 nm (150 nm) / uniform film (80 nm), eps per
+layer drawn with seed 2, harmonics 15x15 (N=225, 450x450 eigenproblems), grids
+256^2, 201 wavelengths in [400, 800] nm, theta=0, TM.  One step = the
+convolution matrices of the stack plus all 201 solves.  Inputs are seeded
+synthetic data of that shape.
+
+  value : solves/s with the grids already resident in HBM
+          (rcwa_geometry_create on device pointers + rcwa_solve_sweep_device)
+  e2e   : solves/s through rcwa_solve_sweep with pinned host buffers
+          (grids H2D and R/T D2H inside the timed region)
+
+Multi-GPU: every rank solves its own copy of the sweep (replicas, no data-path
+collective); value = solves of all ranks / max-over-ranks time.
+
+``--impl reference`` times the CPU port of the reference (the oracle) on the
+host cores instead, one solve per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rcwa-cuda_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "solves/s at |dR|,|dT|<=1e-6 (plain FP64 batched sweep; served mixed-prec vs FP64 reported alongside)"
+UNIT = "solves/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n-lambda", type=int, default=201)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n_lambda):
+    from rcwa_b200 import configs as C
+    return C.c2_sweep(n_lambda=n_lambda)
+
+
+WORKLOAD_DESC = ("3-layer spectral sweep: period 400x400 nm, line grating 120 nm / hole r=100 nm "
+                 "150 nm / uniform film 80 nm, eps seed 2, harmonics 15x15 (N=225, n=450), grids 256^2, "
+                 "201 wavelengths 400-800 nm, theta=0, TM")
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- reference arm
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from helpers_bench import oracle_one_solve
+    pb = workload(args.n_lambda)
+    # bounded sample: one wavelength per step, cycling through non-anomalous points
+    idx = [i for i in range(len(pb.sources)) if i not in (0, 100)]
+    convs = None
+    times = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        convs = oracle_one_solve(pb, idx[(s * 37) % len(idx)], convs)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    tot = sum(times)
+    value = args.steps / tot
+    cores = os.cpu_count()
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD_DESC, "sample": "1 solve per step (conv matrices hoisted after the first)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "1 wavelength of the sweep per step; NumPy/SciPy FP64 restatement, OpenBLAS threads = all host cores"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- ours
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from rcwa_b200 import lib as L
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    pb = workload(args.n_lambda)
+    st, par, srcs = pb.stack, pb.params, pb.sources
+    B = len(srcs)
+    N = (2 * par.nx_harmonics + 1) * (2 * par.ny_harmonics + 1)
+    ctx = L.Context(local)
+    # a dedicated stream: the library launches on it and every CUDA event of
+    # this benchmark is recorded on it
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+
+    # ---- HBM-resident inputs and outputs
+    er_d = torch.from_numpy(st.er.view(np.float64).copy()).cuda()
+    ur_d = torch.from_numpy(st.ur.view(np.float64).copy()).cuda()
+    t_d = torch.from_numpy(st.t.copy()).cuda()
+    R_d = torch.empty(B * N, dtype=torch.float64, device="cuda")
+    T_d = torch.empty(B * N, dtype=torch.float64, device="cuda")
+    tot_d = torch.empty(2 * B, dtype=torch.float64, device="cuda")
+    st_d = torch.empty(B, dtype=torch.int32, device="cuda")
+
+    def step_device():
+        g = ctx.geometry_create(st, par, er_d.data_ptr(), ur_d.data_ptr(), t_d.data_ptr())
+        ctx.solve_sweep_device(g, srcs, L.PREC_FP64, R_d.data_ptr(), T_d.data_ptr(), tot_d.data_ptr(),
+                               st_d.data_ptr())
+        ctx.geometry_destroy(g)   # synchronises the stream
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step_device()
+    barrier()
+
+    L.profile_reset()
+    L.profile_enable(True)
+    l0 = ctx.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_ms = []
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            e_a = torch.cuda.Event(enable_timing=True)
+            e_b = torch.cuda.Event(enable_timing=True)
+            e_a.record(stream)
+            step_device()
+            e_b.record(stream)
+            step_ms.append((e_a, e_b))
+        ev1.record(stream)
+        barrier()
+    L.profile_enable(False)
+    launches = ctx.kernel_launches() - l0
+    dev_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    per_step = [a.elapsed_time(b) for a, b in step_ms]
+    fam = {}
+    for name in ("zgemm", "hess", "formq", "schur", "trevc", "lu_panel"):
+        fam[name] = L.profile_query(name)
+    L.profile_reset()
+    stat_h = st_d.cpu().numpy()
+    R_h = R_d.cpu().numpy().reshape(B, N)
+    tot_h = tot_d.cpu().numpy().reshape(B, 2)
+
+    # ---- end to end through the host-buffer ABI (pinned buffers)
+    er_p = torch.from_numpy(st.er.view(np.float64).copy()).pin_memory()
+    ur_p = torch.from_numpy(st.ur.view(np.float64).copy()).pin_memory()
+    t_p = torch.from_numpy(st.t.copy()).pin_memory()
+    Rh_p = torch.empty((B, N), dtype=torch.float64).pin_memory()
+    Th_p = torch.empty((B, N), dtype=torch.float64).pin_memory()
+    Rn, Tn = Rh_p.numpy(), Th_p.numpy()
+
+    def step_e2e():
+        return ctx.solve_sweep_ptrs(st, par, srcs, L.PREC_FP64, er_p.data_ptr(), ur_p.data_ptr(),
+                                    t_p.data_ptr(), Rn, Tn)
+
+    step_e2e()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_e2e()
+    e1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    h2d = er_p.numel() * 8 + ur_p.numel() * 8 + t_p.numel() * 8 + B * 40
+    d2h = 2 * B * N * 8 + B * 2 * 8 + B * 4
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    # ---- FP64 tensor-pipe peak: cuBLAS ZGEMM measured here (MEASURED_PEAKS.json has no FP64 figure)
+    a = torch.randn(4096, 4096, dtype=torch.complex128, device="cuda")
+    b = torch.randn(4096, 4096, dtype=torch.complex128, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pe0.record()
+    for _ in range(3):
+        torch.matmul(a, b)
+    pe1.record()
+    torch.cuda.synchronize()
+    zgemm_peak = 3 * 8 * 4096 ** 3 / (pe0.elapsed_time(pe1) / 1e3) / 1e12
+    del a, b
+
+    # dominant kernel family by device time
+    dom = max(fam, key=lambda k: fam[k][0])
+    dms, dn, dfl = fam[dom]
+    achieved = (dfl / dn) / (dms / dn / 1e3) / 1e12 if dn and dfl else None
+    shares = {k: round(v[0] / max(1e-9, sum(x[0] for x in fam.values())), 4) for k, v in fam.items()}
+
+    solves = B * args.steps * world
+    value = solves / (dev_ms / 1e3)
+    e2e_val = solves / (e2e_ms / 1e3)
+    clocks = clk.summary()
+
+    cpu = None
+    err = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from helpers_bench import oracle_one_solve_result
+        t0 = time.perf_counter()
+        ref_res = []
+        sample_idx = [26, 167]   # 452 nm and 734 nm (not anomalous)
+        convs = None
+        for i in sample_idx:
+            res, convs = oracle_one_solve_result(pb, i, convs)
+            ref_res.append(res)
+        cpu_t = time.perf_counter() - t0
+        cpu = {"value": len(sample_idx) / cpu_t, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{len(sample_idx)} wavelengths of the sweep (incl. conv matrices once), NumPy/SciPy FP64 restatement, OpenBLAS on all host threads"}
+        err = 0.0
+        for i, res in zip(sample_idx, ref_res):
+            R_gpu = R_h[i].reshape(2 * par.nx_harmonics + 1, 2 * par.ny_harmonics + 1).T
+            err = max(err, float(np.abs(R_gpu - res.R).max()), abs(float(tot_h[i, 1]) - res.T_tot))
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC, "solves_per_step": B, "precision": "fp64",
+                   "parallelism": f"replicas x{world}", "l2": "working set (~17 GB) > L2, no flush needed",
+                   "anomalies": int(((stat_h & L.STATUS_WOOD_ANOMALY) != 0).sum()),
+                   "step_ms_p50": statistics.median(per_step),
+                   "step_ms_p99": float(np.percentile(per_step, 99)),
+                   "max_abs_dR_dT_vs_oracle": err},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": zgemm_peak,
+                     "unit": "TFLOP/s", "frac": (achieved / zgemm_peak) if achieved else None,
+                     "traffic": None,
+                     "peak_source": "cuBLAS ZGEMM 4096^3 (complex128) measured in this run",
+                     "launches": dn, "avg_launch_ms": dms / dn if dn else None,
+                     "family_time_share": shares},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

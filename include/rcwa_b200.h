@@ -1,0 +1,188 @@
+/*
+ * rcwa_b200.h -- C ABI of the B200-native RCWA solve path.
+ *
+ * The reference (rcwa3d/include/rcwa.hpp, rcwa3d/src/rcwa.cpp) exposes its
+ * solver as Eigen-typed C++ free functions sequenced by main()
+ * (rcwa3d/src/main.cpp:111-191).  This header replaces that surface with an
+ * Eigen-free C ABI: plain pointers and sizes, complex128 as {re, im} pairs
+ * (layout-compatible with std::complex<double>), column-major matrices as in
+ * Eigen's default (rcwa.hpp:13), and integer return codes instead of abort()
+ * (rcwa.cpp:300) or std::out_of_range.
+ *
+ * Every entry point returns RCWA_OK (0) or a negative RCWA_ERR_* code; the
+ * message of the last failure on the calling thread is rcwa_last_error().
+ * Numerical trouble inside a solve (singular pivot, eigensolver cap reached,
+ * non-finite output, Kz = 0 at a Rayleigh/Wood anomaly) never aborts: it is
+ * reported in a per-solve status word and the values are left as computed
+ * (Inf/NaN, exactly where the reference would produce them).
+ *
+ * Host-pointer entry points copy inputs to the GPU and results back; the
+ * *_device entry points take device pointers and leave results on the GPU.
+ * A context owns one CUDA stream and its workspace; calls on one context are
+ * serialised, distinct contexts may be used from distinct threads.
+ */
+#ifndef RCWA_B200_H
+#define RCWA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ------------------------------------------------------- */
+#define RCWA_OK 0
+#define RCWA_ERR_INVALID (-1)   /* bad argument (null pointer, size, order) */
+#define RCWA_ERR_CUDA (-2)      /* CUDA runtime error, see rcwa_last_error() */
+#define RCWA_ERR_NOMEM (-3)     /* device allocation failed / over budget */
+#define RCWA_ERR_NUMERIC (-4)   /* at least one per-solve status bit is set */
+#define RCWA_ERR_BUSY (-5)      /* server queue full (back-pressure) */
+#define RCWA_ERR_NOTFOUND (-6)  /* unknown server ticket */
+
+/* ---- per-solve status bits ---------------------------------------------- */
+#define RCWA_STATUS_SINGULAR 1u      /* zero pivot in an LU (rcwa.cpp .lu()) */
+#define RCWA_STATUS_EIG_NOCONV 2u    /* QR iteration cap hit (rcwa.cpp:300 aborts) */
+#define RCWA_STATUS_NONFINITE 4u     /* non-finite R/T */
+#define RCWA_STATUS_WOOD_ANOMALY 8u  /* some Kz == 0: division at rcwa.cpp:225,541,560 */
+
+/* ---- precision modes ---------------------------------------------------- */
+#define RCWA_PREC_FP64 0   /* all-FP64 (parity form, reproduces the reference) */
+#define RCWA_PREC_MIXED 1  /* split-TF32 tensor-core GEMMs + refined FP32 LU; FP64 eig/sqrt/exp/sums */
+
+typedef struct rcwa_complex {
+  double re, im;
+} rcwa_complex;
+
+/* Device (rcwa.hpp:48-78).  er/ur are flat [layer][iy][ix] row-major grids
+ * (rcwa.hpp:56-60, rcwa.cpp:18), t[layer] the thicknesses. */
+typedef struct rcwa_stack {
+  int nx, ny, num_layers;
+  double lx, ly;
+  const rcwa_complex* er;
+  const rcwa_complex* ur;
+  const double* t;
+} rcwa_stack;
+
+/* Source (rcwa.hpp:81-95); k0 = 2*pi/lambda0 is derived (rcwa.hpp:92). */
+typedef struct rcwa_source {
+  double lambda0, theta, phi, pte, ptm;
+} rcwa_source;
+
+/* RCWAParams (rcwa.hpp:98-112).  P = 2*nx_harmonics+1, Q = 2*ny_harmonics+1
+ * (rcwa.cpp:56-58); mode index m = ix*Q + iy (rcwa.cpp:63-64). */
+typedef struct rcwa_params {
+  int nx_harmonics, ny_harmonics;
+  rcwa_complex er_ref, ur_ref, er_trn, ur_trn;
+} rcwa_params;
+
+/* Results (rcwa.hpp:116-128).  R and T are caller-owned Q x P column-major
+ * arrays (Eigen reshaped(Q, P), rcwa.cpp:576, 582). */
+typedef struct rcwa_result {
+  double* R;
+  double* T;
+  double R_tot, T_tot;
+  uint32_t status;
+} rcwa_result;
+
+typedef struct rcwa_context rcwa_context;
+typedef struct rcwa_geometry rcwa_geometry;
+typedef struct rcwa_server rcwa_server;
+
+/* ---- context ------------------------------------------------------------ */
+const char* rcwa_last_error(void);
+int rcwa_version(void);
+int rcwa_context_create(int device, rcwa_context** out);
+int rcwa_context_destroy(rcwa_context* ctx);
+/* Use an external cudaStream_t (NULL restores the context's own stream). */
+int rcwa_context_set_stream(rcwa_context* ctx, void* cuda_stream);
+int rcwa_context_synchronize(rcwa_context* ctx);
+/* Kernels launched by this context since creation (instrumentation). */
+int rcwa_context_kernel_launches(rcwa_context* ctx, uint64_t* count);
+
+/* ---- instrumentation (no reference counterpart: the reference only prints
+ * to stdout, rcwa.cpp:92-156).  When enabled, the hot kernel families
+ * ("zgemm", "hess", "formq", "schur", "trevc", "lu_panel") are bracketed by
+ * CUDA events on their launching stream; query returns summed device time,
+ * launch count and the algorithmic flops of those launches. */
+int rcwa_profile_enable(int on);
+int rcwa_profile_reset(void);
+int rcwa_profile_query(const char* name, double* total_ms, uint64_t* launches, double* flops);
+
+/* ---- end-to-end solve (main.cpp:111-191) -------------------------------- */
+/* One source. */
+int rcwa_solve(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_source* source,
+               const rcwa_params* params, int precision, rcwa_result* out);
+/* Many sources on one stack (wavelength / angle / polarisation sweep), batched
+ * on the GPU.  out[i] receives source i. */
+int rcwa_solve_sweep(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_source* sources,
+                     int n_sources, const rcwa_params* params, int precision,
+                     rcwa_result* out);
+
+/* Geometry handle: the per-layer convolution matrices (main.cpp:125-138,
+ * rcwa.cpp:6-82) built once on the device and reused by every source.  With
+ * stack_on_device != 0 the stack's er/ur/t pointers are device pointers. */
+int rcwa_geometry_create(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_params* params,
+                         int stack_on_device, rcwa_geometry** out);
+int rcwa_geometry_destroy(rcwa_geometry* geom);
+/* Sweep on a prepared geometry.  sources: host array.  R_dev/T_dev: device
+ * arrays [n_sources][Q*P]; tot_dev: device [n_sources][2] (R_tot, T_tot);
+ * status_dev: device uint32 [n_sources].  Asynchronous on the context stream. */
+int rcwa_solve_sweep_device(rcwa_context* ctx, const rcwa_geometry* geom,
+                            const rcwa_source* sources, int n_sources, int precision,
+                            double* R_dev, double* T_dev, double* tot_dev,
+                            uint32_t* status_dev);
+
+/* ---- step-level entry points (host pointers; one per reference function) */
+/* ConvMat, rcwa.cpp:6-82: out is PQ x PQ column-major. */
+int rcwa_convmat(rcwa_context* ctx, const rcwa_complex* field, int layer, int nx, int ny,
+                 int nx_harmonics, int ny_harmonics, rcwa_complex* out);
+/* ComputeWaveVectors, rcwa.cpp:85-160: k_inc[3], Kx/Ky/Kz_ref/Kz_trn[PQ]. */
+int rcwa_wave_vectors(rcwa_context* ctx, double lx, double ly, const rcwa_source* source,
+                      const rcwa_params* params, rcwa_complex* k_inc, rcwa_complex* Kx,
+                      rcwa_complex* Ky, rcwa_complex* Kz_ref, rcwa_complex* Kz_trn);
+/* GapMedium, rcwa.cpp:163-234: W0, V0 are 2PQ x 2PQ. */
+int rcwa_gap_medium(rcwa_context* ctx, int pq, const rcwa_complex* Kx, const rcwa_complex* Ky,
+                    rcwa_complex* W0, rcwa_complex* V0);
+/* SMatrixLayer, rcwa.cpp:254-352 (S21 = S12, S22 = S11, rcwa.cpp:351). */
+int rcwa_smatrix_layer(rcwa_context* ctx, int pq, const rcwa_complex* erc, const rcwa_complex* urc,
+                       const rcwa_complex* Kx, const rcwa_complex* Ky, const rcwa_complex* V0,
+                       double k0, double thickness, rcwa_complex* S11, rcwa_complex* S12,
+                       uint32_t* status);
+/* SMatrixReflection / SMatrixTransmission, rcwa.cpp:354-466 (W_ref = W_trn = I). */
+int rcwa_smatrix_reflection(rcwa_context* ctx, const rcwa_params* params, const rcwa_complex* Kx,
+                            const rcwa_complex* Ky, const rcwa_complex* Kz_ref,
+                            const rcwa_complex* V0, rcwa_complex* S11, rcwa_complex* S12,
+                            rcwa_complex* S21, rcwa_complex* S22);
+int rcwa_smatrix_transmission(rcwa_context* ctx, const rcwa_params* params, const rcwa_complex* Kx,
+                              const rcwa_complex* Ky, const rcwa_complex* Kz_trn,
+                              const rcwa_complex* V0, rcwa_complex* S11, rcwa_complex* S12,
+                              rcwa_complex* S21, rcwa_complex* S22);
+/* RedhefferProduct, rcwa.cpp:588-615: S = A (x) B, all n x n. */
+int rcwa_redheffer(rcwa_context* ctx, int n, const rcwa_complex* const A[4],
+                   const rcwa_complex* const B[4], rcwa_complex* const S[4], uint32_t* status);
+/* ComputeSourceModeCoeff + ComputeReflectedField + ComputeTransmittedField +
+ * ComputeDiffractionEfficiencies, rcwa.cpp:469-585, from S_global's S11/S21. */
+int rcwa_efficiencies(rcwa_context* ctx, const rcwa_source* source, const rcwa_params* params,
+                      const rcwa_complex* k_inc, const rcwa_complex* Kx, const rcwa_complex* Ky,
+                      const rcwa_complex* Kz_ref, const rcwa_complex* Kz_trn,
+                      const rcwa_complex* S11, const rcwa_complex* S21, rcwa_result* out);
+
+/* ---- dense building blocks (batched, host pointers) ---------------------- */
+/* ComplexEigenSolver replacement (rcwa.cpp:298-306): for each of `batch`
+ * n x n matrices A, eigenvalues lam[batch][n] and unit-2-norm eigenvectors
+ * W[batch][n x n].  status[batch] gets RCWA_STATUS_EIG_NOCONV on failure. */
+int rcwa_eig(rcwa_context* ctx, int n, int batch, const rcwa_complex* A, rcwa_complex* lam,
+             rcwa_complex* W, uint32_t* status);
+/* PartialPivLU solve (the .lu().solve calls of rcwa.cpp): X = A^-1 B, batched. */
+int rcwa_lu_solve(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_complex* A,
+                  const rcwa_complex* B, rcwa_complex* X, uint32_t* status);
+/* C = A * B (n x k times k x m), batched; precision selects FP64 or split-TF32. */
+int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_complex* A,
+              const rcwa_complex* B, rcwa_complex* C, int precision);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RCWA_B200_H */

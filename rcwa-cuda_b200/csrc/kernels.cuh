@@ -1,0 +1,112 @@
+// Internal (C++) interface between the kernel files and the solver.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace rcwa {
+
+void count_launch();
+uint64_t launch_count();
+
+// Optional event-pair timing of kernel families (prof.cu).
+bool prof_on();
+void* prof_begin(cudaStream_t s);
+void prof_end(cudaStream_t s, void* tok, const char* name);
+void prof_add_flops(const char* name, double flops);
+
+// ---- dense primitives ------------------------------------------------------
+struct ZGemm {
+  int m = 0, n = 0, k = 0;
+  double2 alpha = {1.0, 0.0}, beta = {0.0, 0.0};
+  const double2* A = nullptr;
+  int lda = 0;
+  long long sA = 0;
+  const double2* B = nullptr;
+  int ldb = 0;
+  long long sB = 0;
+  double2* C = nullptr;
+  int ldc = 0;
+  long long sC = 0;
+  const double2* dl = nullptr;  // optional left (row) scaling, stride sdl per batch
+  long long sdl = 0;
+  const double2* dr = nullptr;  // optional right (column) scaling, stride sdr per batch
+  long long sdr = 0;
+  int batch = 1;
+};
+int zgemm(cudaStream_t s, const ZGemm& g);
+
+// X = A^-1 B on the augmented [A | B] (n x (n+nrhs), column-major, ld >= n).
+int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch,
+          int* piv, uint32_t* status);
+
+// Eigen-decomposition of packed n x n matrices (destroyed).
+size_t zeig_workspace_bytes(int n, int batch);
+int zeig(cudaStream_t s, int n, int batch, double2* A, int ld, long long sA, double2* W,
+         long long sW, double2* lam, long long slam, uint32_t* status, void* ws);
+
+// ---- RCWA building blocks (rcwa_kernels.cu) ---------------------------------
+struct ModeDims {
+  int nxh, nyh, P, Q, N, n;  // N = P*Q, n = 2N
+};
+
+// Convolution matrices of `nl` layer grids (rcwa.cpp:6-82): out[l] is N x N.
+int convmat(cudaStream_t s, const double2* grids, int nl, int nx, int ny, const ModeDims& d,
+            double2* out, double2* scratch);
+size_t convmat_scratch_bytes(int nl, int nx, int ny, const ModeDims& d);
+
+// Per-source wave vectors (rcwa.cpp:85-160) and gap modes (rcwa.cpp:163-234).
+struct SourceDev {
+  double lambda0, theta, phi, pte, ptm;
+};
+struct WaveVecs {
+  double2* Kx;      // [B][N]
+  double2* Ky;      // [B][N]
+  double2* Kzr;     // [B][N]
+  double2* Kzt;     // [B][N]
+  double2* V0;      // [B][4][N]: diagonals (11, 12, 21, 22) of the gap V0
+  double2* kinc;    // [B][4]: k_inc x, y, z, (k0, 0)
+};
+int wave_vectors(cudaStream_t s, const SourceDev* src_dev, int B, double lx, double ly,
+                 const ModeDims& d, double2 er_ref, double2 ur_ref, double2 er_trn,
+                 double2 ur_trn, const WaveVecs& w, uint32_t* status);
+
+// P and Q of a patterned layer (rcwa.cpp:262-286) from erc^-1 / urc^-1.
+int assemble_pq(cudaStream_t s, int B, const ModeDims& d, const double2* erc, const double2* urc,
+                const double2* einv, const double2* uinv, const WaveVecs& w, double2* P,
+                double2* Qm);
+// lam = usqrt(lam2), ilam = 1/lam, X = exp(-k0 t lam) (rcwa.cpp:317, 329, 339).
+int layer_modes(cudaStream_t s, int B, int n, const double2* lam2, const double2* kinc,
+                double t, double2* lam, double2* ilam, double2* X);
+// A = Wi + Vi V0, B = Wi - Vi V0 (rcwa.cpp:335-338); Wi, Vi dense inverses.
+int assemble_ab(cudaStream_t s, int B, const ModeDims& d, const double2* Wi, long long sWi,
+                const double2* Vi, long long sVi, const double2* V0, double2* A, double2* Bm);
+// Uniform-layer S-matrix (analytic modes, W = I), rcwa.cpp:254-352 with
+// erc = eps I, urc = mu I; writes dense S11 and S12.
+int uniform_layer(cudaStream_t s, int B, const ModeDims& d, double2 eps, double2 mu, double t,
+                  const WaveVecs& w, double2* S11, double2* S12, long long sS);
+// Reflection / transmission side S-matrices (rcwa.cpp:354-466), dense.
+int port_smatrix(cudaStream_t s, int B, const ModeDims& d, int side, double2 er, double2 ur,
+                 const WaveVecs& w, double2* S11, double2* S12, double2* S21, double2* S22,
+                 long long sS);
+// Source, fields and efficiencies (rcwa.cpp:469-585) from S_global's S11/S21.
+int efficiencies(cudaStream_t s, int B, const ModeDims& d, const SourceDev* src_dev,
+                 double2 ur_ref, double2 ur_trn, const WaveVecs& w, const double2* S11,
+                 const double2* S21, long long sS, double* R, double* T, double* tot,
+                 uint32_t* status);
+
+int gap_v0(cudaStream_t s, int N, const double2* Kx, const double2* Ky, double2* V0);
+
+// small utilities
+int set_identity(cudaStream_t s, double2* M, int n, int ld, long long stride, int ncols_total,
+                 int col0, int batch, double2 diag);
+int fill_zero(cudaStream_t s, double2* M, size_t count);
+int scale_rows(cudaStream_t s, double2* M, int n, int ncols, int ld, long long stride,
+               const double2* d, long long sd, int batch);
+int copy_blocks(cudaStream_t s, double2* dst, long long sdst, const double2* src, long long ssrc,
+                size_t count, int batch);
+int any_nonuniform(cudaStream_t s, const double2* grid, size_t count, int* flag);
+
+}  // namespace rcwa

@@ -1,0 +1,821 @@
+// Solve orchestration: the reference's main() sequence (main.cpp:111-191)
+// re-planned for a batch of sources on one device.
+//
+//   geometry (once per stack):  ConvMat of every layer's er/ur grid
+//                               (main.cpp:125-138) and, for patterned layers,
+//                               erc^-1 / urc^-1 (the LU of rcwa.cpp:267-281
+//                               is source independent, so it is hoisted).
+//   per chunk of sources:       wave vectors + gap (rcwa.cpp:85-234), then for
+//                               every layer its S-matrix and the star product
+//                               into S_device (main.cpp:146-164), the port
+//                               S-matrices and the two global star products
+//                               (main.cpp:166-170), and the efficiencies
+//                               (main.cpp:182-191).
+// Every dense step is a batched kernel over the chunk (one GEMM / LU / eig
+// launch covers all sources), so the launch count is independent of the
+// number of sources.
+#include <algorithm>
+#include <cstring>
+
+#include "solver.cuh"
+
+namespace rcwa {
+
+int ctx_reserve(rcwa_context* ctx, size_t bytes) {
+  if (bytes <= ctx->ws_bytes) return RCWA_OK;
+  if (ctx->ws) {
+    RCWA_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    RCWA_CUDA_TRY(cudaFree(ctx->ws));
+    ctx->ws = nullptr;
+    ctx->ws_bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&ctx->ws, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error("workspace allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    ctx->ws = nullptr;
+    return RCWA_ERR_NOMEM;
+  }
+  ctx->ws_bytes = bytes;
+  return RCWA_OK;
+}
+
+int ctx_pinned(rcwa_context* ctx, size_t bytes) {
+  if (bytes <= ctx->pinned_bytes) return RCWA_OK;
+  if (ctx->pinned) {
+    RCWA_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    RCWA_CUDA_TRY(cudaFreeHost(ctx->pinned));
+    ctx->pinned = nullptr;
+  }
+  RCWA_CUDA_TRY(cudaMallocHost(&ctx->pinned, bytes));
+  ctx->pinned_bytes = bytes;
+  return RCWA_OK;
+}
+
+static ModeDims dims_of(const rcwa_params* p) {
+  ModeDims d;
+  d.nxh = p->nx_harmonics;
+  d.nyh = p->ny_harmonics;
+  d.P = 2 * d.nxh + 1;
+  d.Q = 2 * d.nyh + 1;
+  d.N = d.P * d.Q;
+  d.n = 2 * d.N;
+  return d;
+}
+
+static double2 c2(const rcwa_complex& c) { return make_double2(c.re, c.im); }
+
+void geometry_free(rcwa_geometry* g) {
+  if (!g) return;
+  if (g->erc) cudaFree(g->erc);
+  if (g->urc) cudaFree(g->urc);
+  if (g->einv) cudaFree(g->einv);
+  if (g->uinv) cudaFree(g->uinv);
+  g->erc = g->urc = g->einv = g->uinv = nullptr;
+}
+
+int geometry_build(rcwa_context* ctx, rcwa_geometry* g, const rcwa_stack* st,
+                   const rcwa_params* p, int on_device) {
+  cudaStream_t s = ctx->stream;
+  const ModeDims d = dims_of(p);
+  g->ctx = ctx;
+  g->d = d;
+  g->nl = st->num_layers;
+  g->nx = st->nx;
+  g->ny = st->ny;
+  g->lx = st->lx;
+  g->ly = st->ly;
+  g->er_ref = c2(p->er_ref);
+  g->ur_ref = c2(p->ur_ref);
+  g->er_trn = c2(p->er_trn);
+  g->ur_trn = c2(p->ur_trn);
+  const int nl = st->num_layers;
+  const size_t G = (size_t)st->nx * st->ny;
+  g->t.assign(nl, 0.0);
+  g->uniform.assign(nl, 0);
+  g->ueps.assign(nl, make_double2(0, 0));
+  g->umu.assign(nl, make_double2(0, 0));
+  const size_t NN = (size_t)d.N * d.N;
+
+  // device copies of the grids (host input) or direct use (device input)
+  const double2* der = nullptr;
+  const double2* dur = nullptr;
+  double2* staging = nullptr;
+  if (on_device) {
+    der = (const double2*)st->er;
+    dur = (const double2*)st->ur;
+    RCWA_CUDA_TRY(cudaMemcpyAsync(g->t.data(), st->t, nl * sizeof(double), cudaMemcpyDeviceToHost, s));
+  } else {
+    std::memcpy(g->t.data(), st->t, nl * sizeof(double));
+  }
+
+  // workspace: staging grids (host case) + convmat scratch + augmented [erc | I]
+  const size_t conv_scr = convmat_scratch_bytes(nl, st->nx, st->ny, d);
+  const size_t stage_b = on_device ? 0 : 2 * (size_t)nl * G * sizeof(double2);
+  const size_t aug_b = (size_t)2 * nl * 2 * NN * sizeof(double2);
+  const size_t piv_b = (size_t)2 * nl * d.N * sizeof(int);
+  const size_t flags_b = 16 * (size_t)nl + 256;
+  int rc = ctx_reserve(ctx, stage_b + conv_scr + aug_b + piv_b + flags_b + 4096);
+  if (rc) return rc;
+  char* w = (char*)ctx->ws;
+  auto take = [&](size_t b) {
+    char* q = w;
+    w += (b + 255) & ~(size_t)255;
+    return q;
+  };
+  if (!on_device) {
+    staging = (double2*)take(stage_b);
+    RCWA_CUDA_TRY(cudaMemcpyAsync(staging, st->er, nl * G * sizeof(double2), cudaMemcpyHostToDevice, s));
+    RCWA_CUDA_TRY(cudaMemcpyAsync(staging + nl * G, st->ur, nl * G * sizeof(double2),
+                                  cudaMemcpyHostToDevice, s));
+    der = staging;
+    dur = staging + nl * G;
+  }
+  double2* scr = (double2*)take(conv_scr);
+  double2* aug = (double2*)take(aug_b);
+  int* piv = (int*)take(piv_b);
+  int* flags = (int*)take(flags_b);
+
+  // uniform layers: both er and ur constant over the grid
+  {
+    RCWA_CUDA_TRY(cudaMemsetAsync(flags, 0, 2 * nl * sizeof(int), s));
+    for (int l = 0; l < nl; ++l) {
+      rc = any_nonuniform(s, der + l * G, G, flags + 2 * l);
+      if (rc) return rc;
+      rc = any_nonuniform(s, dur + l * G, G, flags + 2 * l + 1);
+      if (rc) return rc;
+    }
+    std::vector<int> hf(2 * nl);
+    std::vector<double2> v0(2 * nl);
+    RCWA_CUDA_TRY(cudaMemcpyAsync(hf.data(), flags, 2 * nl * sizeof(int), cudaMemcpyDeviceToHost, s));
+    for (int l = 0; l < nl; ++l) {
+      RCWA_CUDA_TRY(cudaMemcpyAsync(&v0[2 * l], der + l * G, sizeof(double2), cudaMemcpyDeviceToHost, s));
+      RCWA_CUDA_TRY(cudaMemcpyAsync(&v0[2 * l + 1], dur + l * G, sizeof(double2), cudaMemcpyDeviceToHost, s));
+    }
+    RCWA_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int l = 0; l < nl; ++l) {
+      g->uniform[l] = (hf[2 * l] == 0 && hf[2 * l + 1] == 0) ? 1 : 0;
+      g->ueps[l] = v0[2 * l];
+      g->umu[l] = v0[2 * l + 1];
+    }
+  }
+
+  geometry_free(g);
+  RCWA_CUDA_TRY(cudaMalloc(&g->erc, nl * NN * sizeof(double2)));
+  RCWA_CUDA_TRY(cudaMalloc(&g->urc, nl * NN * sizeof(double2)));
+  RCWA_CUDA_TRY(cudaMalloc(&g->einv, nl * NN * sizeof(double2)));
+  RCWA_CUDA_TRY(cudaMalloc(&g->uinv, nl * NN * sizeof(double2)));
+  // ConvMat for er and ur of every layer (main.cpp:126-138)
+  rc = convmat(s, der, nl, st->nx, st->ny, d, g->erc, scr);
+  if (rc) return rc;
+  rc = convmat(s, dur, nl, st->nx, st->ny, d, g->urc, scr);
+  if (rc) return rc;
+  // erc^-1 and urc^-1 of patterned layers: [erc | I] -> [U | erc^-1]
+  std::vector<int> pat;
+  for (int l = 0; l < nl; ++l)
+    if (!g->uniform[l]) pat.push_back(l);
+  const int np = (int)pat.size();
+  if (np > 0) {
+    const long long s2 = 2 * (long long)NN;
+    for (int k = 0; k < np; ++k) {
+      RCWA_CUDA_TRY(cudaMemcpyAsync(aug + k * s2, g->erc + pat[k] * NN, NN * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, s));
+      RCWA_CUDA_TRY(cudaMemcpyAsync(aug + (np + k) * s2, g->urc + pat[k] * NN, NN * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, s));
+    }
+    rc = set_identity(s, aug, d.N, d.N, s2, 2 * d.N, d.N, 2 * np, make_double2(1.0, 0.0));
+    if (rc) return rc;
+    uint32_t* gst = (uint32_t*)(flags + 2 * nl);
+    RCWA_CUDA_TRY(cudaMemsetAsync(gst, 0, 2 * np * sizeof(uint32_t), s));
+    rc = zgesv(s, d.N, d.N, aug, d.N, s2, 2 * np, piv, gst);
+    if (rc) return rc;
+    for (int k = 0; k < np; ++k) {
+      RCWA_CUDA_TRY(cudaMemcpyAsync(g->einv + pat[k] * NN, aug + k * s2 + NN, NN * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, s));
+      RCWA_CUDA_TRY(cudaMemcpyAsync(g->uinv + pat[k] * NN, aug + (np + k) * s2 + NN,
+                                    NN * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  RCWA_CUDA_TRY(cudaStreamSynchronize(s));
+  return RCWA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Redheffer star product A <- A (x) B (rcwa.cpp:588-615), batched.
+//   augFG holds two stacked batches of n x 3n augmented systems:
+//   [I - B11 A22 | B11 | B12] and [I - A22 B11 | A21 | A22].
+// The new S12 is written into `tmp` and the pointers are swapped.
+// ---------------------------------------------------------------------------
+int star_product(rcwa_context* ctx, int B, int n, SMat& A, const SMat& Bm, double2*& tmp,
+                 double2* augFG, int* piv, uint32_t* status) {
+  cudaStream_t s = ctx->stream;
+  const long long nn = (long long)n * n;
+  const long long s3 = 3 * nn;
+  double2* augF = augFG;
+  double2* augG = augFG + (long long)B * s3;
+  int rc;
+  rc = set_identity(s, augF, n, n, s3, 3 * n, 0, B, make_double2(1, 0));
+  if (rc) return rc;
+  rc = set_identity(s, augG, n, n, s3, 3 * n, 0, B, make_double2(1, 0));
+  if (rc) return rc;
+  auto gemm = [&](double2* C, long long sC, const double2* X, long long sX, const double2* Y,
+                  long long sY, double2 alpha, double2 beta) {
+    ZGemm g;
+    g.m = n; g.n = n; g.k = n;
+    g.alpha = alpha; g.beta = beta;
+    g.A = X; g.lda = n; g.sA = sX;
+    g.B = Y; g.ldb = n; g.sB = sY;
+    g.C = C; g.ldc = n; g.sC = sC;
+    g.batch = B;
+    return zgemm(s, g);
+  };
+  const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
+  // F = I - B11 A22 (:602), G = I - A22 B11 (:603)
+  if ((rc = gemm(augF, s3, Bm.p[0], Bm.s[0], A.p[3], A.s[3], mone, one))) return rc;
+  if ((rc = gemm(augG, s3, A.p[3], A.s[3], Bm.p[0], Bm.s[0], mone, one))) return rc;
+  if ((rc = copy_blocks(s, augF + nn, s3, Bm.p[0], Bm.s[0], nn, B))) return rc;
+  if ((rc = copy_blocks(s, augF + 2 * nn, s3, Bm.p[1], Bm.s[1], nn, B))) return rc;
+  if ((rc = copy_blocks(s, augG + nn, s3, A.p[2], A.s[2], nn, B))) return rc;
+  if ((rc = copy_blocks(s, augG + 2 * nn, s3, A.p[3], A.s[3], nn, B))) return rc;
+  // F^-1 [B11 B12], G^-1 [A21 A22] (:605-611), both systems in one batch
+  if ((rc = zgesv(s, n, 2 * n, augFG, n, s3, 2 * B, piv, status))) return rc;
+  // note: status is indexed per system; the caller ORs the two halves.
+  const double2* X1 = augF + nn;      // F^-1 B11
+  const double2* X2 = augF + 2 * nn;  // F^-1 B12
+  const double2* Y1 = augG + nn;      // G^-1 A21
+  const double2* Y2 = augG + 2 * nn;  // G^-1 A22
+  // S11 = A11 + A12 (F^-1 B11) A21 (:608)
+  if ((rc = gemm(tmp, nn, X1, s3, A.p[2], A.s[2], one, zero))) return rc;
+  if ((rc = gemm(A.p[0], A.s[0], A.p[1], A.s[1], tmp, nn, one, one))) return rc;
+  // S21 = B21 (G^-1 A21) (:610) -- A21 is no longer needed
+  if ((rc = gemm(A.p[2], A.s[2], Bm.p[2], Bm.s[2], Y1, s3, one, zero))) return rc;
+  // S22 = B22 + B21 (G^-1 A22) B12 (:611) -- A22 was copied into augG
+  if ((rc = gemm(tmp, nn, Y2, s3, Bm.p[1], Bm.s[1], one, zero))) return rc;
+  if ((rc = copy_blocks(s, A.p[3], A.s[3], Bm.p[3], Bm.s[3], nn, B))) return rc;
+  if ((rc = gemm(A.p[3], A.s[3], Bm.p[2], Bm.s[2], tmp, nn, one, one))) return rc;
+  // S12 = A12 (F^-1 B12) (:609) into tmp, then swap
+  if ((rc = gemm(tmp, nn, A.p[1], A.s[1], X2, s3, one, zero))) return rc;
+  std::swap(A.p[1], tmp);
+  A.s[1] = nn;
+  return RCWA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// workspace plan of one sweep chunk (units: n x n complex blocks per source)
+// ---------------------------------------------------------------------------
+namespace {
+struct Plan {
+  int B;
+  int n, N;
+  // n^2-strided blocks
+  double2* SD[4];
+  double2* tmp;
+  double2* s0;
+  double2* s1;
+  double2* s2;
+  double2* s3;
+  double2* SP[4];   // port S-matrix
+  // augmented
+  double2* augWV;   // [2B] x 2n^2 : [W | I] then [V | I]
+  double2* augA;    // [B] x 2n^2
+  double2* augD;    // [B] x 3n^2
+  double2* augFG;   // [2B] x 3n^2
+  double2* eigws;   // zeig workspace
+  double2* lam2;    // [B][n]
+  double2* lam;     // [B][n]
+  double2* ilam;    // [B][n]
+  double2* X;       // [B][n]
+  WaveVecs wv;
+  SourceDev* src;   // [B]
+  uint32_t* st;     // [3B] scratch status (per system)
+  int* piv;         // [2B][n]
+};
+
+constexpr int kBlocksPerSource = 4 + 1 + 4 + 4 + 4 + 2 + 3 + 6;  // SD,tmp,s0-3,SP,augWV,augA,augD,augFG
+
+size_t plan_bytes(const ModeDims& d, int B) {
+  const size_t nn = (size_t)d.n * d.n;
+  size_t b = (size_t)B * kBlocksPerSource * nn * sizeof(double2);
+  b += zeig_workspace_bytes(d.n, B);
+  b += (size_t)B * 4 * d.n * sizeof(double2);                 // lam2, lam, ilam, X
+  b += (size_t)B * (4 * d.N + 4 * d.N + 4) * sizeof(double2); // Kx Ky Kzr Kzt, V0, kinc
+  b += (size_t)B * sizeof(SourceDev) + (size_t)3 * B * sizeof(uint32_t);
+  b += (size_t)2 * B * d.n * sizeof(int);
+  b += 64 * 256;  // alignment slack
+  return (b + 255) & ~(size_t)255;  // callers place further buffers right after the plan
+}
+
+int plan_take(rcwa_context* ctx, const ModeDims& d, int B, Plan& pl) {
+  int rc = ctx_reserve(ctx, plan_bytes(d, B));
+  if (rc) return rc;
+  char* w = (char*)ctx->ws;
+  auto take = [&](size_t bytes) {
+    char* q = w;
+    w += (bytes + 255) & ~(size_t)255;
+    return q;
+  };
+  const size_t nn = (size_t)d.n * d.n;
+  const size_t blk = (size_t)B * nn * sizeof(double2);
+  pl.B = B;
+  pl.n = d.n;
+  pl.N = d.N;
+  for (int k = 0; k < 4; ++k) pl.SD[k] = (double2*)take(blk);
+  pl.tmp = (double2*)take(blk);
+  pl.s0 = (double2*)take(blk);
+  pl.s1 = (double2*)take(blk);
+  pl.s2 = (double2*)take(blk);
+  pl.s3 = (double2*)take(blk);
+  for (int k = 0; k < 4; ++k) pl.SP[k] = (double2*)take(blk);
+  pl.augWV = (double2*)take(4 * blk);
+  pl.augA = (double2*)take(2 * blk);
+  pl.augD = (double2*)take(3 * blk);
+  pl.augFG = (double2*)take(6 * blk);
+  pl.eigws = (double2*)take(zeig_workspace_bytes(d.n, B));
+  pl.lam2 = (double2*)take((size_t)B * d.n * sizeof(double2));
+  pl.lam = (double2*)take((size_t)B * d.n * sizeof(double2));
+  pl.ilam = (double2*)take((size_t)B * d.n * sizeof(double2));
+  pl.X = (double2*)take((size_t)B * d.n * sizeof(double2));
+  pl.wv.Kx = (double2*)take((size_t)B * d.N * sizeof(double2));
+  pl.wv.Ky = (double2*)take((size_t)B * d.N * sizeof(double2));
+  pl.wv.Kzr = (double2*)take((size_t)B * d.N * sizeof(double2));
+  pl.wv.Kzt = (double2*)take((size_t)B * d.N * sizeof(double2));
+  pl.wv.V0 = (double2*)take((size_t)B * 4 * d.N * sizeof(double2));
+  pl.wv.kinc = (double2*)take((size_t)B * 4 * sizeof(double2));
+  pl.src = (SourceDev*)take((size_t)B * sizeof(SourceDev));
+  pl.st = (uint32_t*)take((size_t)3 * B * sizeof(uint32_t));
+  pl.piv = (int*)take((size_t)2 * B * d.n * sizeof(int));
+  return RCWA_OK;
+}
+
+__global__ void fold_status_kernel(uint32_t* dst, const uint32_t* a, int B, int k) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  uint32_t v = 0;
+  for (int j = 0; j < k; ++j) v |= a[(long long)j * B + b];
+  dst[b] |= v;
+}
+
+int fold_status(cudaStream_t s, uint32_t* dst, const uint32_t* scratch, int B, int k) {
+  fold_status_kernel<<<cdiv_up(B, 128), 128, 0, s>>>(dst, scratch, B, k);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  return RCWA_OK;
+}
+
+// S-matrix of one patterned layer (rcwa.cpp:254-352) for the chunk.
+// Output: S11 at augD[1] (stride 3n^2) and S12 in s2.
+int patterned_layer(rcwa_context* ctx, const rcwa_geometry* g, int l, Plan& pl,
+                    uint32_t* status) {
+  cudaStream_t s = ctx->stream;
+  const ModeDims& d = g->d;
+  const int B = pl.B, n = d.n;
+  const long long nn = (long long)n * n, NN = (long long)d.N * d.N;
+  const long long s2 = 2 * nn, s3 = 3 * nn;
+  const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
+  int rc;
+  // P_i, Q_i (:262-286)
+  if ((rc = assemble_pq(s, B, d, g->erc + l * NN, g->urc + l * NN, g->einv + l * NN,
+                        g->uinv + l * NN, pl.wv, pl.s0, pl.s1)))
+    return rc;
+  // Omega^2 = P Q (:288)
+  ZGemm gm;
+  gm.m = n; gm.n = n; gm.k = n; gm.batch = B;
+  gm.A = pl.s0; gm.lda = n; gm.sA = nn;
+  gm.B = pl.s1; gm.ldb = n; gm.sB = nn;
+  gm.C = pl.s2; gm.ldc = n; gm.sC = nn;
+  if ((rc = zgemm(s, gm))) return rc;
+  // eig (:298-306): W written straight into the first half of [W | I]
+  RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
+  if ((rc = zeig(s, n, B, pl.s2, n, nn, pl.augWV, s2, pl.lam2, n, pl.st, pl.eigws))) return rc;
+  if ((rc = fold_status(s, status, pl.st, B, 1))) return rc;
+  // lambda, 1/lambda, X (:317, :339)
+  if ((rc = layer_modes(s, B, n, pl.lam2, pl.wv.kinc, g->t[l], pl.lam, pl.ilam, pl.X))) return rc;
+  // V = Q W lambda^-1 (:326-330) into the first half of [V | I]
+  double2* augV = pl.augWV + (long long)B * s2;
+  gm = ZGemm();
+  gm.m = n; gm.n = n; gm.k = n; gm.batch = B;
+  gm.A = pl.s1; gm.lda = n; gm.sA = nn;
+  gm.B = pl.augWV; gm.ldb = n; gm.sB = s2;
+  gm.C = augV; gm.ldc = n; gm.sC = s2;
+  gm.dr = pl.ilam; gm.sdr = n;
+  if ((rc = zgemm(s, gm))) return rc;
+  // W^-1, V^-1 (:335-336), one batched solve for both
+  if ((rc = set_identity(s, pl.augWV, n, n, s2, 2 * n, n, 2 * B, one))) return rc;
+  RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
+  if ((rc = zgesv(s, n, n, pl.augWV, n, s2, 2 * B, pl.piv, pl.st))) return rc;
+  if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
+  // A = W^-1 W0 + V^-1 V0 -> s1, B -> s0 (:337-338)
+  if ((rc = assemble_ab(s, B, d, pl.augWV + nn, s2, augV + nn, s2, pl.wv.V0, pl.s1, pl.s0))) return rc;
+  // A^-1 via [A | I]
+  if ((rc = copy_blocks(s, pl.augA, s2, pl.s1, nn, nn, B))) return rc;
+  if ((rc = set_identity(s, pl.augA, n, n, s2, 2 * n, n, B, one))) return rc;
+  RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
+  if ((rc = zgesv(s, n, n, pl.augA, n, s2, B, pl.piv, pl.st))) return rc;
+  if ((rc = fold_status(s, status, pl.st, B, 1))) return rc;
+  const double2* Ai = pl.augA + nn;
+  // T1 = B A^-1 X -> s2   (X diag: column scaling)
+  gm = ZGemm();
+  gm.m = n; gm.n = n; gm.k = n; gm.batch = B;
+  gm.A = pl.s0; gm.lda = n; gm.sA = nn;
+  gm.B = Ai; gm.ldb = n; gm.sB = s2;
+  gm.C = pl.s2; gm.ldc = n; gm.sC = nn;
+  gm.dr = pl.X; gm.sdr = n;
+  if ((rc = zgemm(s, gm))) return rc;
+  // D = A - X T1 B -> augD[0] (:346)
+  if ((rc = copy_blocks(s, pl.augD, s3, pl.s1, nn, nn, B))) return rc;
+  gm = ZGemm();
+  gm.m = n; gm.n = n; gm.k = n; gm.batch = B;
+  gm.alpha = mone; gm.beta = one;
+  gm.A = pl.s2; gm.lda = n; gm.sA = nn;
+  gm.B = pl.s0; gm.ldb = n; gm.sB = nn;
+  gm.C = pl.augD; gm.ldc = n; gm.sC = s3;
+  gm.dl = pl.X; gm.sdl = n;
+  if ((rc = zgemm(s, gm))) return rc;
+  // R1 = X T1 A - B -> augD[1] (:347)
+  if ((rc = copy_blocks(s, pl.augD + nn, s3, pl.s0, nn, nn, B))) return rc;
+  gm.alpha = one; gm.beta = mone;
+  gm.B = pl.s1;
+  gm.C = pl.augD + nn;
+  if ((rc = zgemm(s, gm))) return rc;
+  // identity in augD[2] for D^-1
+  if ((rc = set_identity(s, pl.augD, n, n, s3, 3 * n, 2 * n, B, one))) return rc;
+  // T3 = A^-1 B -> s3 ; R2 = A - B T3 -> s1 (in place) (:348)
+  gm = ZGemm();
+  gm.m = n; gm.n = n; gm.k = n; gm.batch = B;
+  gm.A = Ai; gm.lda = n; gm.sA = s2;
+  gm.B = pl.s0; gm.ldb = n; gm.sB = nn;
+  gm.C = pl.s3; gm.ldc = n; gm.sC = nn;
+  if ((rc = zgemm(s, gm))) return rc;
+  gm.alpha = mone; gm.beta = one;
+  gm.A = pl.s0; gm.sA = nn;
+  gm.B = pl.s3; gm.sB = nn;
+  gm.C = pl.s1;
+  if ((rc = zgemm(s, gm))) return rc;
+  // [D | R1 | I] -> S11 = D^-1 R1, D^-1
+  RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
+  if ((rc = zgesv(s, n, 2 * n, pl.augD, n, s3, B, pl.piv, pl.st))) return rc;
+  if ((rc = fold_status(s, status, pl.st, B, 1))) return rc;
+  // S12 = D^-1 X R2 -> s2
+  if ((rc = scale_rows(s, pl.s1, n, n, n, nn, pl.X, n, B))) return rc;
+  gm = ZGemm();
+  gm.m = n; gm.n = n; gm.k = n; gm.batch = B;
+  gm.A = pl.augD + 2 * nn; gm.lda = n; gm.sA = s3;
+  gm.B = pl.s1; gm.ldb = n; gm.sB = nn;
+  gm.C = pl.s2; gm.ldc = n; gm.sC = nn;
+  (void)zero;
+  return zgemm(s, gm);
+}
+
+}  // namespace
+
+size_t sweep_bytes_per_source(const ModeDims& d) { return plan_bytes(d, 1); }
+
+static int sweep_chunk(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* sources,
+                       int B, double* R, double* T, double* tot, uint32_t* status) {
+  cudaStream_t s = ctx->stream;
+  const ModeDims& d = g->d;
+  const int n = d.n;
+  const long long nn = (long long)n * n, s3 = 3 * nn;
+  Plan pl;
+  int rc = plan_take(ctx, d, B, pl);
+  if (rc) return rc;
+  // sources -> device (through the pinned staging buffer)
+  if ((rc = ctx_pinned(ctx, (size_t)B * sizeof(SourceDev)))) return rc;
+  SourceDev* hs = (SourceDev*)ctx->pinned;
+  RCWA_CUDA_TRY(cudaStreamSynchronize(s));  // staging buffer reuse
+  for (int b = 0; b < B; ++b)
+    hs[b] = SourceDev{sources[b].lambda0, sources[b].theta, sources[b].phi, sources[b].pte, sources[b].ptm};
+  RCWA_CUDA_TRY(cudaMemcpyAsync(pl.src, hs, B * sizeof(SourceDev), cudaMemcpyHostToDevice, s));
+  RCWA_CUDA_TRY(cudaMemsetAsync(status, 0, B * sizeof(uint32_t), s));
+  // wave vectors + gap (main.cpp:140-141)
+  if ((rc = wave_vectors(s, pl.src, B, g->lx, g->ly, d, g->er_ref, g->ur_ref, g->er_trn, g->ur_trn,
+                         pl.wv, status)))
+    return rc;
+  // device S-matrix (main.cpp:143-164)
+  SMat dev;
+  for (int k = 0; k < 4; ++k) {
+    dev.p[k] = pl.SD[k];
+    dev.s[k] = nn;
+  }
+  double2* tmp = pl.tmp;
+  for (int l = 0; l < g->nl; ++l) {
+    SMat lay;
+    if (g->uniform[l]) {
+      // S11 -> s0, S12 -> s1 (sparse content, dense storage)
+      if ((rc = fill_zero(s, pl.s0, (size_t)B * nn))) return rc;
+      if ((rc = fill_zero(s, pl.s1, (size_t)B * nn))) return rc;
+      if ((rc = uniform_layer(s, B, d, g->ueps[l], g->umu[l], g->t[l], pl.wv, pl.s0, pl.s1, nn)))
+        return rc;
+      lay.p[0] = pl.s0; lay.s[0] = nn;
+      lay.p[1] = pl.s1; lay.s[1] = nn;
+    } else {
+      if ((rc = patterned_layer(ctx, g, l, pl, status))) return rc;
+      lay.p[0] = pl.augD + nn; lay.s[0] = s3;
+      lay.p[1] = pl.s2; lay.s[1] = nn;
+    }
+    lay.p[2] = lay.p[1]; lay.s[2] = lay.s[1];   // S21 = S12 (:351)
+    lay.p[3] = lay.p[0]; lay.s[3] = lay.s[0];   // S22 = S11
+    if (l == 0) {
+      // S_init (x) S_layer == S_layer exactly (S11 = S22 = 0, S12 = S21 = I)
+      for (int k = 0; k < 4; ++k)
+        if ((rc = copy_blocks(s, dev.p[k], dev.s[k], lay.p[k], lay.s[k], nn, B))) return rc;
+    } else {
+      RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
+      if ((rc = star_product(ctx, B, n, dev, lay, tmp, pl.augFG, pl.piv, pl.st))) return rc;
+      if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
+    }
+  }
+  if (g->nl == 0) {
+    for (int k = 0; k < 4; ++k) {
+      if ((rc = fill_zero(s, dev.p[k], (size_t)B * nn))) return rc;
+    }
+    if ((rc = set_identity(s, dev.p[1], n, n, nn, n, 0, B, make_double2(1, 0)))) return rc;
+    if ((rc = set_identity(s, dev.p[2], n, n, nn, n, 0, B, make_double2(1, 0)))) return rc;
+  }
+  // S_ref (x) S_device (x) S_trn (main.cpp:166-170)
+  SMat port;
+  for (int k = 0; k < 4; ++k) {
+    port.p[k] = pl.SP[k];
+    port.s[k] = nn;
+    if ((rc = fill_zero(s, pl.SP[k], (size_t)B * nn))) return rc;
+  }
+  if ((rc = port_smatrix(s, B, d, 0, g->er_ref, g->ur_ref, pl.wv, port.p[0], port.p[1], port.p[2],
+                         port.p[3], nn)))
+    return rc;
+  RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
+  if ((rc = star_product(ctx, B, n, port, dev, tmp, pl.augFG, pl.piv, pl.st))) return rc;
+  if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
+  // S_trn into the (now free) device blocks
+  for (int k = 0; k < 4; ++k) {
+    if ((rc = fill_zero(s, dev.p[k], (size_t)B * nn))) return rc;
+  }
+  if ((rc = port_smatrix(s, B, d, 1, g->er_trn, g->ur_trn, pl.wv, dev.p[0], dev.p[1], dev.p[2],
+                         dev.p[3], nn)))
+    return rc;
+  RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
+  if ((rc = star_product(ctx, B, n, port, dev, tmp, pl.augFG, pl.piv, pl.st))) return rc;
+  if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
+  // efficiencies (main.cpp:182-191)
+  return efficiencies(s, B, d, pl.src, g->ur_ref, g->ur_trn, pl.wv, port.p[0], port.p[2], nn, R, T,
+                      tot, status);
+}
+
+int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* sources, int B,
+                 int precision, double* R, double* T, double* tot, uint32_t* status) {
+  if (precision != RCWA_PREC_FP64) {
+    set_last_error("precision mode %d is not available in this build", precision);
+    return RCWA_ERR_INVALID;
+  }
+  if (B <= 0) return RCWA_OK;
+  const ModeDims& d = g->d;
+  // chunk size from the memory budget
+  size_t budget = ctx->mem_budget;
+  if (budget == 0) {
+    size_t fr = 0, totm = 0;
+    RCWA_CUDA_TRY(cudaMemGetInfo(&fr, &totm));
+    budget = (size_t)((fr + ctx->ws_bytes) * 0.6);
+  }
+  const size_t per = plan_bytes(d, 1);
+  int chunk = (int)std::max<size_t>(1, budget / per);
+  chunk = std::min(chunk, B);
+  for (int b0 = 0; b0 < B; b0 += chunk) {
+    const int bc = std::min(chunk, B - b0);
+    const long long N = d.N;
+    int rc = sweep_chunk(ctx, g, sources + b0, bc, R + b0 * N, T + b0 * N, tot + 2LL * b0,
+                         status + b0);
+    if (rc) return rc;
+  }
+  return RCWA_OK;
+}
+
+}  // namespace rcwa
+
+// ===========================================================================
+// Step-level entry points (one reference function each), single problem.
+// ===========================================================================
+namespace rcwa {
+
+namespace {
+struct Arena {
+  char* p;
+  char* take(size_t b) {
+    char* q = p;
+    p += (b + 255) & ~(size_t)255;
+    return q;
+  }
+};
+int h2d(rcwa_context* c, void* d, const void* h, size_t b) {
+  RCWA_CUDA_TRY(cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, c->stream));
+  return RCWA_OK;
+}
+int d2h(rcwa_context* c, void* h, const void* d, size_t b) {
+  RCWA_CUDA_TRY(cudaMemcpyAsync(h, d, b, cudaMemcpyDeviceToHost, c->stream));
+  return RCWA_OK;
+}
+ModeDims dims_n(int N) {
+  ModeDims d{};
+  d.N = N;
+  d.n = 2 * N;
+  d.P = N;  // only N / n are used by the per-mode kernels
+  d.Q = 1;
+  return d;
+}
+}  // namespace
+
+int step_wave_vectors(rcwa_context* ctx, double lx, double ly, const rcwa_source* src,
+                      const rcwa_params* p, double2* kinc, double2* Kx, double2* Ky, double2* Kzr,
+                      double2* Kzt, double2* V0d) {
+  const ModeDims d = dims_of(p);
+  const size_t N = d.N;
+  int rc = ctx_reserve(ctx, (8 * N + 4) * 16 + 64 + 8 * 256);
+  if (rc) return rc;
+  Arena a{(char*)ctx->ws};
+  WaveVecs w;
+  w.Kx = (double2*)a.take(N * 16);
+  w.Ky = (double2*)a.take(N * 16);
+  w.Kzr = (double2*)a.take(N * 16);
+  w.Kzt = (double2*)a.take(N * 16);
+  w.V0 = (double2*)a.take(4 * N * 16);
+  w.kinc = (double2*)a.take(4 * 16);
+  SourceDev* ds = (SourceDev*)a.take(sizeof(SourceDev));
+  uint32_t* st = (uint32_t*)a.take(4);
+  SourceDev hs{src->lambda0, src->theta, src->phi, src->pte, src->ptm};
+  if ((rc = h2d(ctx, ds, &hs, sizeof(hs)))) return rc;
+  RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 4, ctx->stream));
+  if ((rc = wave_vectors(ctx->stream, ds, 1, lx, ly, d, c2(p->er_ref), c2(p->ur_ref), c2(p->er_trn),
+                         c2(p->ur_trn), w, st)))
+    return rc;
+  if ((rc = d2h(ctx, Kx, w.Kx, N * 16)) || (rc = d2h(ctx, Ky, w.Ky, N * 16)) ||
+      (rc = d2h(ctx, Kzr, w.Kzr, N * 16)) || (rc = d2h(ctx, Kzt, w.Kzt, N * 16)) ||
+      (rc = d2h(ctx, V0d, w.V0, 4 * N * 16)) || (rc = d2h(ctx, kinc, w.kinc, 4 * 16)))
+    return rc;
+  RCWA_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return RCWA_OK;
+}
+
+int step_gap_v0(rcwa_context* ctx, int N, const double2* Kx, const double2* Ky, double2* V0d) {
+  int rc = ctx_reserve(ctx, (size_t)6 * N * 16 + 1024);
+  if (rc) return rc;
+  Arena a{(char*)ctx->ws};
+  double2* dKx = (double2*)a.take((size_t)N * 16);
+  double2* dKy = (double2*)a.take((size_t)N * 16);
+  double2* dV = (double2*)a.take((size_t)4 * N * 16);
+  if ((rc = h2d(ctx, dKx, Kx, (size_t)N * 16)) || (rc = h2d(ctx, dKy, Ky, (size_t)N * 16))) return rc;
+  if ((rc = gap_v0(ctx->stream, N, dKx, dKy, dV))) return rc;
+  if ((rc = d2h(ctx, V0d, dV, (size_t)4 * N * 16))) return rc;
+  RCWA_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return RCWA_OK;
+}
+
+int step_smatrix_layer(rcwa_context* ctx, int N, const double2* erc, const double2* urc,
+                       const double2* Kx, const double2* Ky, const double2* V0d, double k0,
+                       double t, double2* S11, double2* S12, uint32_t* status) {
+  const ModeDims d = dims_n(N);
+  const size_t NN = (size_t)N * N, nn = (size_t)d.n * d.n;
+  const size_t extra = 8 * NN * 16 + 2 * NN * 16 * 2 + 2 * (size_t)N * 4 + 1024 + 16 * 256;
+  int rc = ctx_reserve(ctx, plan_bytes(d, 1) + extra);
+  if (rc) return rc;
+  Plan pl;
+  if ((rc = plan_take(ctx, d, 1, pl))) return rc;
+  Arena a{(char*)ctx->ws + ((plan_bytes(d, 1) + 255) & ~(size_t)255)};
+  rcwa_geometry g;
+  g.ctx = ctx;
+  g.d = d;
+  g.nl = 1;
+  g.t = {t};
+  g.uniform = {0};
+  g.erc = (double2*)a.take(NN * 16);
+  g.urc = (double2*)a.take(NN * 16);
+  g.einv = (double2*)a.take(NN * 16);
+  g.uinv = (double2*)a.take(NN * 16);
+  double2* aug = (double2*)a.take(4 * NN * 16);
+  int* piv = (int*)a.take(2 * (size_t)N * 4);
+  uint32_t* dst = (uint32_t*)a.take(16);
+  cudaStream_t s = ctx->stream;
+  if ((rc = h2d(ctx, g.erc, erc, NN * 16)) || (rc = h2d(ctx, g.urc, urc, NN * 16))) return rc;
+  RCWA_CUDA_TRY(cudaMemcpyAsync(aug, g.erc, NN * 16, cudaMemcpyDeviceToDevice, s));
+  RCWA_CUDA_TRY(cudaMemcpyAsync(aug + 2 * NN, g.urc, NN * 16, cudaMemcpyDeviceToDevice, s));
+  if ((rc = set_identity(s, aug, N, N, 2 * NN, 2 * N, N, 2, make_double2(1, 0)))) return rc;
+  RCWA_CUDA_TRY(cudaMemsetAsync(dst, 0, 16, s));
+  if ((rc = zgesv(s, N, N, aug, N, 2 * NN, 2, piv, dst))) return rc;
+  RCWA_CUDA_TRY(cudaMemcpyAsync(g.einv, aug + NN, NN * 16, cudaMemcpyDeviceToDevice, s));
+  RCWA_CUDA_TRY(cudaMemcpyAsync(g.uinv, aug + 3 * NN, NN * 16, cudaMemcpyDeviceToDevice, s));
+  double2 kinc[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(k0, 0)};
+  if ((rc = h2d(ctx, pl.wv.Kx, Kx, (size_t)N * 16)) || (rc = h2d(ctx, pl.wv.Ky, Ky, (size_t)N * 16)) ||
+      (rc = h2d(ctx, pl.wv.V0, V0d, (size_t)4 * N * 16)) || (rc = h2d(ctx, pl.wv.kinc, kinc, sizeof(kinc))))
+    return rc;
+  if ((rc = patterned_layer(ctx, &g, 0, pl, dst))) return rc;
+  if ((rc = d2h(ctx, S11, pl.augD + nn, nn * 16)) || (rc = d2h(ctx, S12, pl.s2, nn * 16))) return rc;
+  uint32_t hs[2] = {0, 0};
+  if ((rc = d2h(ctx, hs, dst, 8))) return rc;
+  RCWA_CUDA_TRY(cudaStreamSynchronize(s));
+  *status = hs[0] | hs[1];
+  g.erc = g.urc = g.einv = g.uinv = nullptr;  // arena memory, not owned
+  return RCWA_OK;
+}
+
+int step_port(rcwa_context* ctx, int side, int N, double2 er, double2 ur, const double2* Kx,
+              const double2* Ky, const double2* Kz, const double2* V0d, double2* S[4]) {
+  const ModeDims d = dims_n(N);
+  const size_t nn = (size_t)d.n * d.n;
+  int rc = ctx_reserve(ctx, 4 * nn * 16 + (size_t)8 * N * 16 + 64 + 16 * 256);
+  if (rc) return rc;
+  Arena a{(char*)ctx->ws};
+  double2* dS[4];
+  for (int k = 0; k < 4; ++k) dS[k] = (double2*)a.take(nn * 16);
+  WaveVecs w;
+  w.Kx = (double2*)a.take((size_t)N * 16);
+  w.Ky = (double2*)a.take((size_t)N * 16);
+  w.Kzr = (double2*)a.take((size_t)N * 16);
+  w.Kzt = w.Kzr;
+  w.V0 = (double2*)a.take((size_t)4 * N * 16);
+  w.kinc = (double2*)a.take(64);
+  cudaStream_t s = ctx->stream;
+  if ((rc = h2d(ctx, w.Kx, Kx, (size_t)N * 16)) || (rc = h2d(ctx, w.Ky, Ky, (size_t)N * 16)) ||
+      (rc = h2d(ctx, w.Kzr, Kz, (size_t)N * 16)) || (rc = h2d(ctx, w.V0, V0d, (size_t)4 * N * 16)))
+    return rc;
+  for (int k = 0; k < 4; ++k)
+    if ((rc = fill_zero(s, dS[k], nn))) return rc;
+  if ((rc = port_smatrix(s, 1, d, side, er, ur, w, dS[0], dS[1], dS[2], dS[3], (long long)nn))) return rc;
+  for (int k = 0; k < 4; ++k)
+    if ((rc = d2h(ctx, S[k], dS[k], nn * 16))) return rc;
+  RCWA_CUDA_TRY(cudaStreamSynchronize(s));
+  return RCWA_OK;
+}
+
+int step_redheffer(rcwa_context* ctx, int n, const double2* const A[4], const double2* const B[4],
+                   double2* const S[4], uint32_t* status) {
+  const size_t nn = (size_t)n * n;
+  int rc = ctx_reserve(ctx, (9 + 6) * nn * 16 + 2 * (size_t)n * 4 + 64 + 20 * 256);
+  if (rc) return rc;
+  Arena a{(char*)ctx->ws};
+  SMat dA, dB;
+  for (int k = 0; k < 4; ++k) {
+    dA.p[k] = (double2*)a.take(nn * 16);
+    dA.s[k] = (long long)nn;
+    dB.p[k] = (double2*)a.take(nn * 16);
+    dB.s[k] = (long long)nn;
+    if ((rc = h2d(ctx, dA.p[k], A[k], nn * 16)) || (rc = h2d(ctx, dB.p[k], B[k], nn * 16))) return rc;
+  }
+  double2* tmp = (double2*)a.take(nn * 16);
+  double2* augFG = (double2*)a.take(6 * nn * 16);
+  int* piv = (int*)a.take(2 * (size_t)n * 4);
+  uint32_t* st = (uint32_t*)a.take(16);
+  RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 16, ctx->stream));
+  if ((rc = star_product(ctx, 1, n, dA, dB, tmp, augFG, piv, st))) return rc;
+  for (int k = 0; k < 4; ++k)
+    if ((rc = d2h(ctx, S[k], dA.p[k], nn * 16))) return rc;
+  uint32_t hs[2] = {0, 0};
+  if ((rc = d2h(ctx, hs, st, 8))) return rc;
+  RCWA_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  *status = hs[0] | hs[1];
+  return RCWA_OK;
+}
+
+int step_efficiencies(rcwa_context* ctx, const rcwa_source* src, const rcwa_params* p,
+                      const double2* kinc, const double2* Kx, const double2* Ky,
+                      const double2* Kzr, const double2* Kzt, const double2* S11,
+                      const double2* S21, rcwa_result* out) {
+  const ModeDims d = dims_of(p);
+  const size_t N = d.N, nn = (size_t)d.n * d.n;
+  int rc = ctx_reserve(ctx, 2 * nn * 16 + 8 * N * 16 + 4 * N * 8 + 1024 + 16 * 256);
+  if (rc) return rc;
+  Arena a{(char*)ctx->ws};
+  double2* dS11 = (double2*)a.take(nn * 16);
+  double2* dS21 = (double2*)a.take(nn * 16);
+  WaveVecs w;
+  w.Kx = (double2*)a.take(N * 16);
+  w.Ky = (double2*)a.take(N * 16);
+  w.Kzr = (double2*)a.take(N * 16);
+  w.Kzt = (double2*)a.take(N * 16);
+  w.V0 = nullptr;
+  w.kinc = (double2*)a.take(64);
+  double* dR = (double*)a.take(N * 8);
+  double* dT = (double*)a.take(N * 8);
+  double* dtot = (double*)a.take(16);
+  uint32_t* st = (uint32_t*)a.take(4);
+  SourceDev* ds = (SourceDev*)a.take(sizeof(SourceDev));
+  SourceDev hs{src->lambda0, src->theta, src->phi, src->pte, src->ptm};
+  double2 ki[4] = {kinc[0], kinc[1], kinc[2], make_double2(2.0 * 3.14159265358979323846 / src->lambda0, 0)};
+  if ((rc = h2d(ctx, dS11, S11, nn * 16)) || (rc = h2d(ctx, dS21, S21, nn * 16)) ||
+      (rc = h2d(ctx, w.Kx, Kx, N * 16)) || (rc = h2d(ctx, w.Ky, Ky, N * 16)) ||
+      (rc = h2d(ctx, w.Kzr, Kzr, N * 16)) || (rc = h2d(ctx, w.Kzt, Kzt, N * 16)) ||
+      (rc = h2d(ctx, w.kinc, ki, sizeof(ki))) || (rc = h2d(ctx, ds, &hs, sizeof(hs))))
+    return rc;
+  RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 4, ctx->stream));
+  if ((rc = efficiencies(ctx->stream, 1, d, ds, c2(p->ur_ref), c2(p->ur_trn), w, dS11, dS21,
+                         (long long)nn, dR, dT, dtot, st)))
+    return rc;
+  double htot[2];
+  uint32_t hst = 0;
+  if (out->R && (rc = d2h(ctx, out->R, dR, N * 8))) return rc;
+  if (out->T && (rc = d2h(ctx, out->T, dT, N * 8))) return rc;
+  if ((rc = d2h(ctx, htot, dtot, 16)) || (rc = d2h(ctx, &hst, st, 4))) return rc;
+  RCWA_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  out->R_tot = htot[0];
+  out->T_tot = htot[1];
+  out->status = hst;
+  return RCWA_OK;
+}
+
+}  // namespace rcwa

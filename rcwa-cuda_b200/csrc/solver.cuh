@@ -1,0 +1,66 @@
+// Host-side solver objects behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "kernels.cuh"
+
+struct rcwa_context {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  // grow-only device arena for per-call workspace
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  // small pinned host staging buffer
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+  uint64_t launches_at_create = 0;
+  size_t mem_budget = 0;  // bytes usable for one sweep chunk (0 = auto)
+};
+
+struct rcwa_geometry {
+  rcwa_context* ctx = nullptr;
+  rcwa::ModeDims d{};
+  int nl = 0, nx = 0, ny = 0;
+  double lx = 0, ly = 0;
+  std::vector<double> t;
+  std::vector<char> uniform;
+  std::vector<double2> ueps, umu;  // grid value of uniform layers
+  double2 er_ref{}, ur_ref{}, er_trn{}, ur_trn{};
+  double2* erc = nullptr;   // [nl][N*N]
+  double2* urc = nullptr;
+  double2* einv = nullptr;  // [nl][N*N], patterned layers only
+  double2* uinv = nullptr;
+};
+
+namespace rcwa {
+
+int ctx_reserve(rcwa_context* ctx, size_t bytes);
+int ctx_pinned(rcwa_context* ctx, size_t bytes);
+
+// Build convolution matrices and their inverses.  grids_er/ur are device
+// pointers ([nl][ny][nx]) when on_device, host pointers otherwise.
+int geometry_build(rcwa_context* ctx, rcwa_geometry* g, const rcwa_stack* st,
+                   const rcwa_params* p, int on_device);
+void geometry_free(rcwa_geometry* g);
+
+// Sweep over sources (host array) on a prepared geometry; outputs on device.
+int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* sources, int B,
+                 int precision, double* R, double* T, double* tot, uint32_t* status);
+
+// Bytes of device workspace per source for a sweep at this size.
+size_t sweep_bytes_per_source(const ModeDims& d);
+
+// Dense building blocks on device pointers (used by the step-level ABI).
+struct SMat {
+  double2* p[4];
+  long long s[4];
+};
+int star_product(rcwa_context* ctx, int B, int n, SMat& A, const SMat& Bm, double2*& tmp,
+                 double2* augFG, int* piv, uint32_t* status);
+
+}  // namespace rcwa

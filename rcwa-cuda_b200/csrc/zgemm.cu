@@ -1,0 +1,148 @@
+// Batched complex128 GEMM on FP64 CUDA cores.
+//
+//   C[b] = alpha * diag(dl[b]) * A[b] * B[b] * diag(dr[b]) + beta * C[b]
+//
+// Column-major, arbitrary m/n/k/ld/batch strides.  This is the dense
+// contraction behind every Eigen operator* of the reference's S-matrix algebra
+// (rcwa.cpp:288, 326, 346-348, 602-611).  The optional diagonal scalings fold
+// the reference's asDiagonal() products (rcwa.cpp:273-285, 329, 339) into the
+// epilogue so no dense diagonal matrix is ever materialised.
+//
+// Tiling: 64x64 C tile per CTA, K step 8, 256 threads as 16x16, each thread a
+// 4x4 complex micro-tile (rows tx+16i, cols ty+16j so that warp stores are
+// coalesced along the column).  A and B tiles are staged into shared memory
+// with cp.async (16-byte copies, zero-filled outside the matrix) and double
+// buffered.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace rcwa {
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 8, NT = 256;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
+  unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
+  int src_bytes = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(gmem),
+               "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__global__ void __launch_bounds__(NT, 2)
+zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, int lda,
+             long long sA, const double2* __restrict__ B, int ldb, long long sB, double2 beta,
+             double2* __restrict__ C, int ldc, long long sC, const double2* __restrict__ dl,
+             long long sdl, const double2* __restrict__ dr, long long sdr) {
+  __shared__ __align__(16) double2 As[2][BK][BM];
+  __shared__ __align__(16) double2 Bs[2][BK][BN];
+
+  const int b = blockIdx.z;
+  A += (long long)b * sA;
+  B += (long long)b * sB;
+  C += (long long)b * sC;
+  const int m0 = blockIdx.y * BM;
+  const int n0 = blockIdx.x * BN;
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+
+  double2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = cmk(0.0, 0.0);
+
+  auto load_tile = [&](int buf, int k0) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int e = tid + h * NT;
+      // A tile: 64 rows x 8 k
+      int r = e & 63, kk = e >> 6;
+      int gr = m0 + r, gk = k0 + kk;
+      bool pa = (gr < m) && (gk < k);
+      const double2* srcA = pa ? (A + (long long)gk * lda + gr) : A;
+      cp_async16(&As[buf][kk][r], srcA, pa);
+      // B tile: 8 k x 64 cols
+      int kb = e & 7, c = e >> 3;
+      int gk2 = k0 + kb, gc = n0 + c;
+      bool pb = (gk2 < k) && (gc < n);
+      const double2* srcB = pb ? (B + (long long)gc * ldb + gk2) : B;
+      cp_async16(&Bs[buf][kb][c], srcB, pb);
+    }
+    cp_async_commit();
+  };
+
+  const int ktiles = (k + BK - 1) / BK;
+  if (ktiles > 0) load_tile(0, 0);
+  for (int t = 0; t < ktiles; ++t) {
+    const int buf = t & 1;
+    if (t + 1 < ktiles) {
+      load_tile(buf ^ 1, (t + 1) * BK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      double2 a[4], bb[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bb[j] = Bs[buf][kk][ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cfma(acc[i][j], a[i], bb[j]);
+    }
+    __syncthreads();
+  }
+
+  const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    int col = n0 + ty + 16 * j;
+    if (col >= n) continue;
+    double2 sr = dr ? dr[(long long)b * sdr + col] : cmk(1.0, 0.0);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      int row = m0 + tx + 16 * i;
+      if (row >= m) continue;
+      double2 v = cmul(alpha, acc[i][j]);
+      if (dl) v = cmul(dl[(long long)b * sdl + row], v);
+      if (dr) v = cmul(v, sr);
+      double2* cp = C + (long long)col * ldc + row;
+      if (use_beta) v = cadd(v, cmul(beta, *cp));
+      *cp = v;
+    }
+  }
+}
+
+}  // namespace
+
+int zgemm(cudaStream_t s, const ZGemm& g) {
+  if (g.m <= 0 || g.n <= 0 || g.batch <= 0) return RCWA_OK;
+  if (g.k <= 0) {
+    // C = beta*C: reuse the kernel with k = 0 (acc stays 0).
+  }
+  dim3 grid(cdiv_up(g.n, BN), cdiv_up(g.m, BM), g.batch);
+  void* tok = prof_begin(s);
+  zgemm_kernel<<<grid, NT, 0, s>>>(g.m, g.n, g.k < 0 ? 0 : g.k, g.alpha, g.A, g.lda, g.sA, g.B,
+                                   g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, g.dr,
+                                   g.sdr);
+  prof_end(s, tok, "zgemm");
+  if (tok) {
+    // algorithmic flops of this launch, for the roofline (8 m n k per matrix)
+    prof_add_flops("zgemm", 8.0 * g.m * (double)g.n * (double)(g.k < 0 ? 0 : g.k) * g.batch);
+  }
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  return RCWA_OK;
+}
+
+}  // namespace rcwa

@@ -1,0 +1,276 @@
+// Batched complex128 linear solve X = A^-1 B by LU with partial pivoting.
+//
+// This replaces every Eigen ``.lu().solve(...)`` (PartialPivLU) of the
+// reference (rcwa.cpp:267, 270, 280, 281, 335, 336, 345-348, 392-408,
+// 453-462, 520, 605-611).  The system is stored as one augmented column-major
+// block M = [A | B] (n rows, n + nrhs columns); on return the A part holds U
+// (and the L multipliers) and the B part holds the solution.
+//
+// Blocked right-looking elimination with panel width NB:
+//   panel   : one CTA per matrix factors the n-j x NB panel (pivot search,
+//             row swaps inside the panel, scaling, rank-1 updates);
+//   swap+L  : one thread per trailing column applies the panel's row swaps and
+//             the unit-lower NB x NB forward substitution (U12 = L11^-1 A12);
+//   update  : the trailing block [A22 | B2] -= L21 * [U12 | Y1] runs as a
+//             batched GEMM (zgemm), which carries almost all the flops.
+// Back substitution with U runs block-wise: NB x NB upper solve per block,
+// then a GEMM update of the rows above.
+//
+// Row swaps are applied to the trailing columns only: L is consumed on the fly
+// by the right-hand sides, so the columns left of the panel are never needed.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace rcwa {
+
+namespace {
+
+constexpr int NB = 32;
+constexpr int PANEL_NT = 256;
+constexpr int COL_NT = 64;
+
+__device__ __forceinline__ void argmax_reduce(double& v, int& idx) {
+  // warp-level: keep the larger value, ties -> smaller index
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    double ov = __shfl_down_sync(0xffffffffu, v, off);
+    int oi = __shfl_down_sync(0xffffffffu, idx, off);
+    if (ov > v || (ov == v && oi < idx)) {
+      v = ov;
+      idx = oi;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(PANEL_NT)
+lu_panel_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int j, int jb,
+                int* __restrict__ pivg, uint32_t* __restrict__ status) {
+  const int b = blockIdx.x;
+  double2* M = Mg + (long long)b * stride;
+  int* piv = pivg + (long long)b * n;
+  __shared__ double s_val[PANEL_NT / 32];
+  __shared__ int s_idx[PANEL_NT / 32];
+  __shared__ double2 s_urow[NB];
+  __shared__ int s_p;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+
+  for (int c = 0; c < jb; ++c) {
+    const int col = j + c;
+    double2* Mc = M + (long long)col * ld;
+    // 1. pivot search over rows col..n-1 (|re|+|im|, first maximum wins)
+    double best = -1.0;
+    int bi = n;
+    for (int r = col + tid; r < n; r += PANEL_NT) {
+      double v = cabs1(Mc[r]);
+      if (v > best) { best = v; bi = r; }
+    }
+    argmax_reduce(best, bi);
+    if (lane == 0) { s_val[wid] = best; s_idx[wid] = bi; }
+    __syncthreads();
+    if (wid == 0) {
+      best = lane < PANEL_NT / 32 ? s_val[lane] : -1.0;
+      bi = lane < PANEL_NT / 32 ? s_idx[lane] : n;
+      argmax_reduce(best, bi);
+      if (lane == 0) {
+        if (bi >= n) bi = col;
+        s_p = bi;
+        piv[col] = bi;
+      }
+    }
+    __syncthreads();
+    const int p = s_p;
+    // 2. swap rows col <-> p inside the panel
+    if (p != col) {
+      for (int cc = tid; cc < jb; cc += PANEL_NT) {
+        double2* q = M + (long long)(j + cc) * ld;
+        double2 t = q[col];
+        q[col] = q[p];
+        q[p] = t;
+      }
+    }
+    __syncthreads();
+    // 3. pivot row of the remaining panel columns -> smem
+    for (int cc = c + 1 + tid; cc < jb; cc += PANEL_NT) s_urow[cc] = M[(long long)(j + cc) * ld + col];
+    const double2 pv = Mc[col];
+    if (tid == 0 && pv.x == 0.0 && pv.y == 0.0) atomicOr(status + b, (unsigned)ST_SINGULAR);
+    __syncthreads();
+    const double2 inv = crcp(pv);
+    // 4. scale the column below the pivot and rank-1 update the panel
+    for (int r = col + 1 + tid; r < n; r += PANEL_NT) {
+      double2 l = cmul(Mc[r], inv);
+      Mc[r] = l;
+      for (int cc = c + 1; cc < jb; ++cc) {
+        double2* q = M + (long long)(j + cc) * ld + r;
+        double2 u = s_urow[cc];
+        double2 v = *q;
+        v.x -= l.x * u.x - l.y * u.y;
+        v.y -= l.x * u.y + l.y * u.x;
+        *q = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Row swaps of panel j plus forward substitution with the unit-lower L11 for
+// columns [c_begin, c_end) of the augmented matrix.
+__global__ void __launch_bounds__(COL_NT)
+lu_swap_lsolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int j, int jb,
+                      int c_begin, int c_end, const int* __restrict__ pivg) {
+  const int b = blockIdx.y;
+  double2* M = Mg + (long long)b * stride;
+  const int* piv = pivg + (long long)b * n;
+  __shared__ double2 L[NB][NB + 1];  // L[r][c]
+  __shared__ int sp[NB];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < jb * jb; e += COL_NT) {
+    int r = e % jb, c = e / jb;
+    L[r][c] = M[(long long)(j + c) * ld + j + r];
+  }
+  for (int e = tid; e < jb; e += COL_NT) sp[e] = piv[j + e];
+  __syncthreads();
+  const int col = c_begin + blockIdx.x * COL_NT + tid;
+  if (col >= c_end) return;
+  double2* q = M + (long long)col * ld;
+  for (int c = 0; c < jb; ++c) {
+    int p = sp[c];
+    if (p != j + c) {
+      double2 t = q[j + c];
+      q[j + c] = q[p];
+      q[p] = t;
+    }
+  }
+  double2 x[NB];
+#pragma unroll
+  for (int c = 0; c < NB; ++c) x[c] = (c < jb) ? q[j + c] : cmk(0.0, 0.0);
+#pragma unroll
+  for (int c = 0; c < NB; ++c) {
+#pragma unroll
+    for (int r = c + 1; r < NB; ++r) {
+      if (r < jb) {
+        double2 l = L[r][c];
+        x[r].x -= l.x * x[c].x - l.y * x[c].y;
+        x[r].y -= l.x * x[c].y + l.y * x[c].x;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NB; ++c)
+    if (c < jb) q[j + c] = x[c];
+}
+
+// Upper-triangular solve X = U11^-1 X for rows j..j+jb-1 of the right-hand
+// side columns [c_begin, c_end).
+__global__ void __launch_bounds__(COL_NT)
+lu_usolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int j, int jb, int c_begin,
+                 int c_end) {
+  const int b = blockIdx.y;
+  double2* M = Mg + (long long)b * stride;
+  __shared__ double2 U[NB][NB + 1];
+  __shared__ double2 dinv[NB];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < jb * jb; e += COL_NT) {
+    int r = e % jb, c = e / jb;
+    U[r][c] = M[(long long)(j + c) * ld + j + r];
+  }
+  __syncthreads();
+  for (int e = tid; e < jb; e += COL_NT) dinv[e] = crcp(U[e][e]);
+  __syncthreads();
+  const int col = c_begin + blockIdx.x * COL_NT + tid;
+  if (col >= c_end) return;
+  double2* q = M + (long long)col * ld;
+  double2 x[NB];
+#pragma unroll
+  for (int c = 0; c < NB; ++c) x[c] = (c < jb) ? q[j + c] : cmk(0.0, 0.0);
+#pragma unroll
+  for (int c = NB - 1; c >= 0; --c) {
+    if (c < jb) {
+      x[c] = cmul(x[c], dinv[c]);
+#pragma unroll
+      for (int r = 0; r < c; ++r) {
+        double2 u = U[r][c];
+        x[r].x -= u.x * x[c].x - u.y * x[c].y;
+        x[r].y -= u.x * x[c].y + u.y * x[c].x;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NB; ++c)
+    if (c < jb) q[j + c] = x[c];
+}
+
+}  // namespace
+
+int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch,
+          int* piv, uint32_t* status) {
+  if (n <= 0 || batch <= 0) return RCWA_OK;
+  const int ncols = n + nrhs;
+  for (int j = 0; j < n; j += NB) {
+    const int jb = (n - j < NB) ? (n - j) : NB;
+    void* tok = prof_begin(s);
+    lu_panel_kernel<<<batch, PANEL_NT, 0, s>>>(M, ld, stride, n, j, jb, piv, status);
+    prof_end(s, tok, "lu_panel");
+    count_launch();
+    RCWA_LAUNCH_CHECK();
+    const int cb = j + jb;
+    if (cb < ncols) {
+      dim3 g(cdiv_up(ncols - cb, COL_NT), batch);
+      lu_swap_lsolve_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, jb, cb, ncols, piv);
+      count_launch();
+      RCWA_LAUNCH_CHECK();
+      if (cb < n) {
+        ZGemm gm;
+        gm.m = n - cb;
+        gm.n = ncols - cb;
+        gm.k = jb;
+        gm.alpha = cmk(-1.0, 0.0);
+        gm.beta = cmk(1.0, 0.0);
+        gm.A = M + (long long)j * ld + cb;
+        gm.lda = ld;
+        gm.sA = stride;
+        gm.B = M + (long long)cb * ld + j;
+        gm.ldb = ld;
+        gm.sB = stride;
+        gm.C = M + (long long)cb * ld + cb;
+        gm.ldc = ld;
+        gm.sC = stride;
+        gm.batch = batch;
+        int rc = zgemm(s, gm);
+        if (rc) return rc;
+      }
+    }
+  }
+  if (nrhs <= 0) return RCWA_OK;
+  const int nblk = (n + NB - 1) / NB;
+  for (int bi = nblk - 1; bi >= 0; --bi) {
+    const int j = bi * NB;
+    const int jb = (n - j < NB) ? (n - j) : NB;
+    dim3 g(cdiv_up(nrhs, COL_NT), batch);
+    lu_usolve_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, j, jb, n, ncols);
+    count_launch();
+    RCWA_LAUNCH_CHECK();
+    if (j > 0) {
+      ZGemm gm;
+      gm.m = j;
+      gm.n = nrhs;
+      gm.k = jb;
+      gm.alpha = cmk(-1.0, 0.0);
+      gm.beta = cmk(1.0, 0.0);
+      gm.A = M + (long long)j * ld;
+      gm.lda = ld;
+      gm.sA = stride;
+      gm.B = M + (long long)n * ld + j;
+      gm.ldb = ld;
+      gm.sB = stride;
+      gm.C = M + (long long)n * ld;
+      gm.ldc = ld;
+      gm.sC = stride;
+      gm.batch = batch;
+      int rc = zgemm(s, gm);
+      if (rc) return rc;
+    }
+  }
+  return RCWA_OK;
+}
+
+}  // namespace rcwa

@@ -1,0 +1,49 @@
+"""The C-ABI library loads and exports every symbol include/rcwa_b200.h
+declares (CPU only: no compute call is made)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "rcwa_b200.h")
+
+
+def _declared():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    names = re.findall(r"\b(rcwa_[a-z0-9_]+)\s*\(", txt)
+    return sorted(set(names))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from rcwa_b200 import build as B
+    if not os.path.exists(B.LIB_PATH):
+        B.build()
+    return ctypes.CDLL(B.LIB_PATH)
+
+
+def test_header_declares_entry_points():
+    names = _declared()
+    for must in ("rcwa_solve", "rcwa_solve_sweep", "rcwa_convmat", "rcwa_eig", "rcwa_lu_solve",
+                 "rcwa_redheffer", "rcwa_smatrix_layer", "rcwa_efficiencies"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    missing = [n for n in _declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header():
+    from rcwa_b200 import lib as L
+    assert set(_declared()) <= set(L.declared_symbols()) | set(getattr(L, "EXTRA_SYMBOLS", []))
+
+
+def test_last_error_without_gpu(lib):
+    lib.rcwa_last_error.restype = ctypes.c_char_p
+    assert isinstance(lib.rcwa_last_error(), bytes)
+    lib.rcwa_version.restype = ctypes.c_int
+    assert lib.rcwa_version() >= 10000
