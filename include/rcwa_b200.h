@@ -174,6 +174,31 @@ int rcwa_efficiencies(rcwa_context* ctx, const rcwa_source* source, const rcwa_p
  * W[batch][n x n].  status[batch] gets RCWA_STATUS_EIG_NOCONV on failure. */
 int rcwa_eig(rcwa_context* ctx, int n, int batch, const rcwa_complex* A, rcwa_complex* lam,
              rcwa_complex* W, uint32_t* status);
+/* Allocation-free eigensolver.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory -- code recording a CUDA
+ * graph, latency-critical loops that must keep away from the allocator, or
+ * hosts that give this library a fixed memory budget -- this runs the same
+ * eigensolver as rcwa_eig with no cudaMalloc/cudaFree and no allocating
+ * library call.  All pointers are DEVICE pointers: A_dev (batch packed n x n,
+ * column-major, left unchanged), lam_dev (batch x n), W_dev (batch packed
+ * n x n), status_dev (batch uint32, cleared by the call).  Work is queued on
+ * cuda_stream (NULL = legacy default stream); the call does not synchronise.
+ *
+ * Scratch lives in one fixed device array of RCWA_EIG_NOALLOC_SCRATCH_BYTES
+ * compiled into the library, which every GPU that loads the library holds
+ * until the process exits.  Limits: n <= RCWA_EIG_NOALLOC_MAX_N and
+ * batch * (3 n^2 + n) * 16 bytes (plus alignment) within the scratch size,
+ * otherwise RCWA_ERR_INVALID with the limit in rcwa_last_error().  The first
+ * call on a device looks up the array's device address once (with that
+ * device current); make that first call before any stream capture.  All calls
+ * share the one array, which keeps the last call's contents: calls whose GPU
+ * work overlaps (different streams, or several host threads) race on it and
+ * must be serialised by the caller. */
+#define RCWA_EIG_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
+#define RCWA_EIG_NOALLOC_MAX_N 128
+int rcwa_eig_noalloc(int n, int batch, const rcwa_complex* A_dev, rcwa_complex* lam_dev,
+                     rcwa_complex* W_dev, uint32_t* status_dev, void* cuda_stream);
 /* PartialPivLU solve (the .lu().solve calls of rcwa.cpp): X = A^-1 B, batched. */
 int rcwa_lu_solve(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_complex* A,
                   const rcwa_complex* B, rcwa_complex* X, uint32_t* status);

@@ -16,6 +16,7 @@ bool prof_on();
 void* prof_begin(cudaStream_t s);
 void prof_end(cudaStream_t s, void* tok, const char* name);
 void prof_add_flops(const char* name, double flops);
+void prof_suspend(bool on);
 
 // ---- dense primitives ------------------------------------------------------
 struct ZGemm {

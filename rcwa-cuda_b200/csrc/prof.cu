@@ -36,10 +36,16 @@ cudaEvent_t get_event() {
 }
 }  // namespace
 
-bool prof_on() { return g_on; }
+static thread_local int t_suspend = 0;
+
+bool prof_on() { return g_on && t_suspend == 0; }
+
+// Calls that must not create any CUDA object suspend event recording on their
+// thread for their duration.
+void prof_suspend(bool on) { t_suspend += on ? 1 : -1; }
 
 void* prof_begin(cudaStream_t s) {
-  if (!g_on) return nullptr;
+  if (!g_on || t_suspend) return nullptr;
   std::lock_guard<std::mutex> lk(g_mu);
   cudaEvent_t e = get_event();
   cudaEventRecord(e, s);

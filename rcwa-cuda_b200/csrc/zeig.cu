@@ -28,6 +28,7 @@
 // Non-finite input is detected up front and reported as NONFINITE|EIG_NOCONV
 // without iterating.
 #include <cfloat>
+#include <mutex>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -657,4 +658,84 @@ int zeig(cudaStream_t s, int n, int batch, double2* A, int ld, long long sA, dou
   return RCWA_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free eigensolver entry point.
+//
+// Some callers cannot allocate device memory: code running inside a CUDA
+// graph that is being captured, real-time loops that must not touch the
+// allocator, and hosts that hand this library a fixed memory budget up front.
+// For them rcwa_eig_noalloc runs the same eigensolver as rcwa_eig, but its
+// scratch (a copy of the input, the Schur vectors Z, the triangular
+// eigenvectors X and the Householder scalars) lives in the file-scope device
+// array below instead of a cudaMalloc'd workspace.  The array is part of the
+// library image: every GPU that loads the library holds its
+// RCWA_EIG_NOALLOC_SCRATCH_BYTES until the process exits.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_eig_noalloc_scratch[RCWA_EIG_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+}  // namespace
+
+// Device address of the scratch array on the current device, looked up once
+// per device (cudaGetSymbolAddress with that device current).
+static int noalloc_scratch(void** out) {
+  int dev = 0;
+  RCWA_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_last_error("rcwa_eig_noalloc: device %d out of range", dev);
+    return RCWA_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_eig_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_last_error("rcwa_eig_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+      return RCWA_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return RCWA_OK;
+}
+
+size_t eig_noalloc_bytes(int n, int batch) {
+  const size_t copy = (size_t)batch * n * n * sizeof(double2);
+  return ((copy + 255) & ~(size_t)255) + zeig_workspace_bytes(n, batch);
+}
+
 }  // namespace rcwa
+
+extern "C" int rcwa_eig_noalloc(int n, int batch, const rcwa_complex* A_dev, rcwa_complex* lam_dev,
+                                rcwa_complex* W_dev, uint32_t* status_dev, void* cuda_stream) {
+  using namespace rcwa;
+  if (n <= 0 || batch <= 0 || !A_dev || !lam_dev || !W_dev || !status_dev) {
+    set_last_error("rcwa_eig_noalloc: bad argument");
+    return RCWA_ERR_INVALID;
+  }
+  if (n > RCWA_EIG_NOALLOC_MAX_N || eig_noalloc_bytes(n, batch) > RCWA_EIG_NOALLOC_SCRATCH_BYTES) {
+    set_last_error("rcwa_eig_noalloc: n=%d batch=%d needs %zu scratch bytes; the fixed scratch holds "
+                   "%zu bytes and n may not exceed %d",
+                   n, batch, eig_noalloc_bytes(n, batch), (size_t)RCWA_EIG_NOALLOC_SCRATCH_BYTES,
+                   RCWA_EIG_NOALLOC_MAX_N);
+    return RCWA_ERR_INVALID;
+  }
+  void* base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)cuda_stream;
+  const size_t nn = (size_t)n * n;
+  double2* Acopy = (double2*)base;
+  void* ws = (char*)base + ((batch * nn * sizeof(double2) + 255) & ~(size_t)255);
+  // the kernels OR status bits into status_dev: it must start at zero
+  RCWA_CUDA_TRY(cudaMemsetAsync(status_dev, 0, (size_t)batch * sizeof(uint32_t), s));
+  RCWA_CUDA_TRY(cudaMemcpyAsync(Acopy, A_dev, batch * nn * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+  prof_suspend(true);
+  rc = zeig(s, n, batch, Acopy, n, (long long)nn, (double2*)W_dev, (long long)nn, (double2*)lam_dev, n,
+            status_dev, ws);
+  prof_suspend(false);
+  return rc;
+}

@@ -99,6 +99,7 @@ _SIGS = {
     "rcwa_efficiencies": ([_VP, C.POINTER(CSource), C.POINTER(CParams), _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                            C.POINTER(CResult)], C.c_int),
     "rcwa_eig": ([_VP, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
+    "rcwa_eig_noalloc": ([C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_lu_solve": ([_VP, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_gemm": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, C.c_int], C.c_int),
 }
