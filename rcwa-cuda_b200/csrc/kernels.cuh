@@ -86,17 +86,30 @@ int assemble_ab(cudaStream_t s, int B, const ModeDims& d, const double2* Wi, lon
                 const double2* Vi, long long sVi, const double2* V0, double2* A, double2* Bm);
 // Uniform-layer S-matrix (analytic modes, W = I), rcwa.cpp:254-352 with
 // erc = eps I, urc = mu I; writes dense S11 and S12.
+// bd != 0 writes the 2x2-block-diagonal "BD" form: per block four diagonals
+// [X(i,i), X(i,i+N), X(i+N,i), X(i+N,i+N)] of length N (4N values).
 int uniform_layer(cudaStream_t s, int B, const ModeDims& d, double2 eps, double2 mu, double t,
-                  const WaveVecs& w, double2* S11, double2* S12, long long sS);
-// Reflection / transmission side S-matrices (rcwa.cpp:354-466), dense.
+                  const WaveVecs& w, double2* S11, double2* S12, long long sS, int bd);
+// Reflection / transmission side S-matrices (rcwa.cpp:354-466), dense or BD.
 int port_smatrix(cudaStream_t s, int B, const ModeDims& d, int side, double2 er, double2 ur,
                  const WaveVecs& w, double2* S11, double2* S12, double2* S21, double2* S22,
-                 long long sS);
-// Source, fields and efficiencies (rcwa.cpp:469-585) from S_global's S11/S21.
+                 long long sS, int bd);
+// Source, fields and efficiencies (rcwa.cpp:469-585) from S_global's S11/S21
+// (full n x n blocks, or compact: only the two source columns, n x 2).
 int efficiencies(cudaStream_t s, int B, const ModeDims& d, const SourceDev* src_dev,
                  double2 ur_ref, double2 ur_trn, const WaveVecs& w, const double2* S11,
-                 const double2* S21, long long sS, double* R, double* T, double* tot,
+                 const double2* S21, long long sS, int compact, double* R, double* T, double* tot,
                  uint32_t* status);
+// C = beta C + alpha (X M) (side 0) or (M X) (side 1) [+ I], X in BD form.
+int bd_apply(cudaStream_t s, int side, int N, int rows, int cols, const double2* X, long long sX,
+             const double2* M, int ldm, long long sM, double2* C, int ldc, long long sC,
+             double2 alpha, double2 beta, int addI, int batch);
+// C[:, 0:2] = beta C + alpha X[:, (a, a+N)], X in BD form.
+int bd_cols(cudaStream_t s, int N, int a, const double2* X, long long sX, double2* C, int ldc,
+            long long sC, double2 alpha, double2 beta, int batch);
+// C = X (dense expansion) or C += X (accumulate), X in BD form.
+int bd_dense(cudaStream_t s, int N, const double2* X, long long sX, double2* C, long long sC,
+             int accumulate, int batch);
 
 int gap_v0(cudaStream_t s, int N, const double2* Kx, const double2* Ky, double2* V0);
 

@@ -304,6 +304,19 @@ __device__ __forceinline__ void store22(double2* M, int n, int N, int i, const C
   M[(long long)(i + N) * n + i + N] = x.d;
 }
 
+// "BD" storage of a 2x2-block-diagonal n x n block X: four diagonals
+// [X(i,i), X(i,i+N), X(i+N,i), X(i+N,i+N)], each of length N.
+__device__ __forceinline__ void store22x(double2* M, int n, int N, int i, const C22& x, bool bd) {
+  if (bd) {
+    M[i] = x.a;
+    M[N + i] = x.b;
+    M[2 * N + i] = x.c;
+    M[3 * N + i] = x.d;
+  } else {
+    store22(M, n, N, i, x);
+  }
+}
+
 __device__ __forceinline__ C22 gap_v0(const double2* V0, int N, int i) {
   return m22(V0[i], V0[N + i], V0[2 * N + i], V0[3 * N + i]);
 }
@@ -314,7 +327,7 @@ __device__ __forceinline__ C22 gap_v0(const double2* V0, int N, int i) {
 // invariant to the choice of basis inside the degenerate pairs.
 __global__ void uniform_layer_kernel(int N, double2 eps, double2 mu, double t, WaveVecs w,
                                      double2* __restrict__ S11g, double2* __restrict__ S12g,
-                                     long long sS) {
+                                     long long sS, int bd) {
   const int b = blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
@@ -341,15 +354,15 @@ __global__ void uniform_layer_kernel(int N, double2 eps, double2 mu, double t, W
   const C22 Di = minv(D);
   const C22 S11 = mmul(Di, msub(mscale(mmul(BAi, A), x2), B));          // :347
   const C22 S12 = mscale(mmul(Di, msub(A, mmul(BAi, B))), x);           // :348
-  store22(S11g + (long long)b * sS, n, N, i, S11);
-  store22(S12g + (long long)b * sS, n, N, i, S12);
+  store22x(S11g + (long long)b * sS, n, N, i, S11, bd);
+  store22x(S12g + (long long)b * sS, n, N, i, S12, bd);
 }
 
 // Reflection (side 0, rcwa.cpp:354-411) / transmission (side 1, :414-466).
 __global__ void port_smatrix_kernel(int N, int side, double2 er, double2 ur, WaveVecs w,
                                     double2* __restrict__ S11g, double2* __restrict__ S12g,
                                     double2* __restrict__ S21g, double2* __restrict__ S22g,
-                                    long long sS) {
+                                    long long sS, int bd) {
   const int b = blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
@@ -374,15 +387,87 @@ __global__ void port_smatrix_kernel(int N, int side, double2 er, double2 ur, Wav
   const C22 mAiB = mscale(AiB, cmk(-1.0, 0.0));
   const long long ob = (long long)b * sS;
   if (side == 0) {   // :405-408
-    store22(S11g + ob, n, N, i, mAiB);
-    store22(S12g + ob, n, N, i, two);
-    store22(S21g + ob, n, N, i, half);
-    store22(S22g + ob, n, N, i, BAi);
+    store22x(S11g + ob, n, N, i, mAiB, bd);
+    store22x(S12g + ob, n, N, i, two, bd);
+    store22x(S21g + ob, n, N, i, half, bd);
+    store22x(S22g + ob, n, N, i, BAi, bd);
   } else {           // :460-463
-    store22(S11g + ob, n, N, i, BAi);
-    store22(S12g + ob, n, N, i, half);
-    store22(S21g + ob, n, N, i, two);
-    store22(S22g + ob, n, N, i, mAiB);
+    store22x(S11g + ob, n, N, i, BAi, bd);
+    store22x(S12g + ob, n, N, i, half, bd);
+    store22x(S21g + ob, n, N, i, two, bd);
+    store22x(S22g + ob, n, N, i, mAiB, bd);
+  }
+}
+
+// ---- products with BD blocks (O(n^2) instead of a dense GEMM) --------------
+// C = beta C + alpha (X M) [side 0]  or  beta C + alpha (M X) [side 1], plus I
+// when addI; X is BD, M and C dense (column-major, rows x cols).
+__global__ void bd_apply_kernel(int side, int N, int rows, int cols, const double2* __restrict__ Xg,
+                                long long sX, const double2* __restrict__ Mg, int ldm, long long sM,
+                                double2* __restrict__ Cg, int ldc, long long sC, double2 alpha,
+                                double2 beta, int addI) {
+  const int b = blockIdx.y;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)rows * cols) return;
+  const int i = (int)(e % rows), j = (int)(e / rows);
+  const double2* X = Xg + (long long)b * sX;
+  const double2* M = Mg + (long long)b * sM;
+  double2 v;
+  if (side == 0) {
+    const int ii = i < N ? i : i - N;
+    const double2 m0 = M[(long long)j * ldm + ii], m1 = M[(long long)j * ldm + ii + N];
+    v = i < N ? cadd(cmul(X[ii], m0), cmul(X[N + ii], m1))
+              : cadd(cmul(X[2 * N + ii], m0), cmul(X[3 * N + ii], m1));
+  } else {
+    const int jj = j < N ? j : j - N;
+    const double2 m0 = M[(long long)jj * ldm + i], m1 = M[(long long)(jj + N) * ldm + i];
+    v = j < N ? cadd(cmul(m0, X[jj]), cmul(m1, X[2 * N + jj]))
+              : cadd(cmul(m0, X[N + jj]), cmul(m1, X[3 * N + jj]));
+  }
+  v = cmul(alpha, v);
+  if (addI && i == j) v.x += 1.0;
+  double2* c = Cg + (long long)b * sC + (long long)j * ldc + i;
+  if (beta.x != 0.0 || beta.y != 0.0) v = cadd(v, cmul(beta, *c));
+  *c = v;
+}
+
+// C[:, 0:2] = beta C + alpha X[:, (a, a+N)] for a BD block X (dense n x 2 out).
+__global__ void bd_cols_kernel(int N, int a, const double2* __restrict__ Xg, long long sX,
+                               double2* __restrict__ Cg, int ldc, long long sC, double2 alpha,
+                               double2 beta) {
+  const int b = blockIdx.y;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = 2 * N;
+  if (e >= 2 * n) return;
+  const int i = e % n, j = e / n;
+  const double2* X = Xg + (long long)b * sX;
+  double2 v = cmk(0.0, 0.0);
+  if (i == a) v = j == 0 ? X[a] : X[N + a];
+  else if (i == a + N) v = j == 0 ? X[2 * N + a] : X[3 * N + a];
+  v = cmul(alpha, v);
+  double2* c = Cg + (long long)b * sC + (long long)j * ldc + i;
+  if (beta.x != 0.0 || beta.y != 0.0) v = cadd(v, cmul(beta, *c));
+  *c = v;
+}
+
+// C (dense n x n) = beta C + X (BD): only the four diagonals are touched when
+// beta == 1; with beta == 0 the whole block is written.
+__global__ void bd_dense_kernel(int N, const double2* __restrict__ Xg, long long sX,
+                                double2* __restrict__ Cg, long long sC, int accumulate) {
+  const int b = blockIdx.y;
+  const int n = 2 * N;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)n * n) return;
+  const int i = (int)(e % n), j = (int)(e / n);
+  const double2* X = Xg + (long long)b * sX;
+  const int ii = i < N ? i : i - N, jj = j < N ? j : j - N;
+  double2 v = cmk(0.0, 0.0);
+  if (ii == jj) v = X[(i >= N ? 2 : 0) * N + (j >= N ? N : 0) + ii];
+  double2* c = Cg + (long long)b * sC + e;
+  if (accumulate) {
+    if (ii == jj) *c = cadd(*c, v);
+  } else {
+    *c = v;
   }
 }
 
@@ -398,7 +483,7 @@ __device__ void normalize3(double2 v[3]) {
 
 __global__ void efficiencies_kernel(int N, const SourceDev* __restrict__ srcs, double2 ur_ref,
                                     double2 ur_trn, WaveVecs w, const double2* __restrict__ S11g,
-                                    const double2* __restrict__ S21g, long long sS,
+                                    const double2* __restrict__ S21g, long long sS, int compact,
                                     double* __restrict__ Rg, double* __restrict__ Tg,
                                     double* __restrict__ tot, uint32_t* __restrict__ status) {
   const int b = blockIdx.x;
@@ -427,7 +512,9 @@ __global__ void efficiencies_kernel(int N, const SourceDev* __restrict__ srcs, d
   }
   __syncthreads();
   const double2 c1 = s_pol[0], c2 = s_pol[1];          // esrc at PQ/2 and PQ/2+PQ; csrc = esrc (W_ref = I)
-  const int src0 = N / 2, src1 = N / 2 + N;
+  // columns PQ/2 and PQ/2+PQ of S11/S21, or columns 0/1 when only those two
+  // columns were formed (compact n x 2 storage)
+  const int src0 = compact ? 0 : N / 2, src1 = compact ? 1 : N / 2 + N;
   const double2* S11 = S11g + (long long)b * sS;
   const double2* S21 = S21g + (long long)b * sS;
   const double den = cdiv(ki[2], ur_ref).x;
@@ -604,8 +691,9 @@ int assemble_ab(cudaStream_t s, int B, const ModeDims& d, const double2* Wi, lon
 }
 
 int uniform_layer(cudaStream_t s, int B, const ModeDims& d, double2 eps, double2 mu, double t,
-                  const WaveVecs& w, double2* S11, double2* S12, long long sS) {
-  uniform_layer_kernel<<<dim3(cdiv_up(d.N, 128), B), 128, 0, s>>>(d.N, eps, mu, t, w, S11, S12, sS);
+                  const WaveVecs& w, double2* S11, double2* S12, long long sS, int bd) {
+  uniform_layer_kernel<<<dim3(cdiv_up(d.N, 128), B), 128, 0, s>>>(d.N, eps, mu, t, w, S11, S12, sS,
+                                                                   bd);
   count_launch();
   RCWA_LAUNCH_CHECK();
   return RCWA_OK;
@@ -613,9 +701,9 @@ int uniform_layer(cudaStream_t s, int B, const ModeDims& d, double2 eps, double2
 
 int port_smatrix(cudaStream_t s, int B, const ModeDims& d, int side, double2 er, double2 ur,
                  const WaveVecs& w, double2* S11, double2* S12, double2* S21, double2* S22,
-                 long long sS) {
+                 long long sS, int bd) {
   port_smatrix_kernel<<<dim3(cdiv_up(d.N, 128), B), 128, 0, s>>>(d.N, side, er, ur, w, S11, S12,
-                                                                  S21, S22, sS);
+                                                                  S21, S22, sS, bd);
   count_launch();
   RCWA_LAUNCH_CHECK();
   return RCWA_OK;
@@ -623,10 +711,38 @@ int port_smatrix(cudaStream_t s, int B, const ModeDims& d, int side, double2 er,
 
 int efficiencies(cudaStream_t s, int B, const ModeDims& d, const SourceDev* src_dev,
                  double2 ur_ref, double2 ur_trn, const WaveVecs& w, const double2* S11,
-                 const double2* S21, long long sS, double* R, double* T, double* tot,
+                 const double2* S21, long long sS, int compact, double* R, double* T, double* tot,
                  uint32_t* status) {
-  efficiencies_kernel<<<B, 256, 0, s>>>(d.N, src_dev, ur_ref, ur_trn, w, S11, S21, sS, R, T, tot,
-                                         status);
+  efficiencies_kernel<<<B, 256, 0, s>>>(d.N, src_dev, ur_ref, ur_trn, w, S11, S21, sS, compact, R, T,
+                                         tot, status);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  return RCWA_OK;
+}
+
+int bd_apply(cudaStream_t s, int side, int N, int rows, int cols, const double2* X, long long sX,
+             const double2* M, int ldm, long long sM, double2* C, int ldc, long long sC,
+             double2 alpha, double2 beta, int addI, int batch) {
+  const long long ne = (long long)rows * cols;
+  bd_apply_kernel<<<dim3(cdiv_up(ne, 256), batch), 256, 0, s>>>(side, N, rows, cols, X, sX, M, ldm, sM,
+                                                                 C, ldc, sC, alpha, beta, addI);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  return RCWA_OK;
+}
+
+int bd_cols(cudaStream_t s, int N, int a, const double2* X, long long sX, double2* C, int ldc,
+            long long sC, double2 alpha, double2 beta, int batch) {
+  bd_cols_kernel<<<dim3(cdiv_up(4 * N, 256), batch), 256, 0, s>>>(N, a, X, sX, C, ldc, sC, alpha, beta);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  return RCWA_OK;
+}
+
+int bd_dense(cudaStream_t s, int N, const double2* X, long long sX, double2* C, long long sC,
+             int accumulate, int batch) {
+  const long long nn = 4LL * N * N;
+  bd_dense_kernel<<<dim3(cdiv_up(nn, 256), batch), 256, 0, s>>>(N, X, sX, C, sC, accumulate);
   count_launch();
   RCWA_LAUNCH_CHECK();
   return RCWA_OK;

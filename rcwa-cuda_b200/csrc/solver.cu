@@ -274,7 +274,8 @@ struct Plan {
   double2* s1;
   double2* s2;
   double2* s3;
-  double2* SP[4];   // port S-matrix
+  double2* pbd;     // [B] x 32N: BD reflection (16N) then transmission (16N) S-matrix
+  double2* lbd;     // [B] x 8N: BD S11, S12 of a uniform layer
   // augmented
   double2* augWV;   // [2B] x 2n^2 : [W | I] then [V | I]
   double2* augA;    // [B] x 2n^2
@@ -291,11 +292,12 @@ struct Plan {
   int* piv;         // [2B][n]
 };
 
-constexpr int kBlocksPerSource = 4 + 1 + 4 + 4 + 4 + 2 + 3 + 6;  // SD,tmp,s0-3,SP,augWV,augA,augD,augFG
+constexpr int kBlocksPerSource = 4 + 1 + 4 + 4 + 2 + 3 + 6;  // SD,tmp,s0-3,augWV,augA,augD,augFG
 
 size_t plan_bytes(const ModeDims& d, int B) {
   const size_t nn = (size_t)d.n * d.n;
   size_t b = (size_t)B * kBlocksPerSource * nn * sizeof(double2);
+  b += (size_t)B * 40 * d.N * sizeof(double2);                // pbd, lbd
   b += zeig_workspace_bytes(d.n, B);
   b += (size_t)B * 4 * d.n * sizeof(double2);                 // lam2, lam, ilam, X
   b += (size_t)B * (4 * d.N + 4 * d.N + 4) * sizeof(double2); // Kx Ky Kzr Kzt, V0, kinc
@@ -325,7 +327,8 @@ int plan_take(rcwa_context* ctx, const ModeDims& d, int B, Plan& pl) {
   pl.s1 = (double2*)take(blk);
   pl.s2 = (double2*)take(blk);
   pl.s3 = (double2*)take(blk);
-  for (int k = 0; k < 4; ++k) pl.SP[k] = (double2*)take(blk);
+  pl.pbd = (double2*)take((size_t)B * 32 * d.N * sizeof(double2));
+  pl.lbd = (double2*)take((size_t)B * 8 * d.N * sizeof(double2));
   pl.augWV = (double2*)take(4 * blk);
   pl.augA = (double2*)take(2 * blk);
   pl.augD = (double2*)take(3 * blk);
@@ -437,8 +440,6 @@ int patterned_layer(rcwa_context* ctx, const rcwa_geometry* g, int l, Plan& pl,
   gm.B = pl.s1;
   gm.C = pl.augD + nn;
   if ((rc = zgemm(s, gm))) return rc;
-  // identity in augD[2] for D^-1
-  if ((rc = set_identity(s, pl.augD, n, n, s3, 3 * n, 2 * n, B, one))) return rc;
   // T3 = A^-1 B -> s3 ; R2 = A - B T3 -> s1 (in place) (:348)
   gm = ZGemm();
   gm.m = n; gm.n = n; gm.k = n; gm.batch = B;
@@ -451,19 +452,127 @@ int patterned_layer(rcwa_context* ctx, const rcwa_geometry* g, int l, Plan& pl,
   gm.B = pl.s3; gm.sB = nn;
   gm.C = pl.s1;
   if ((rc = zgemm(s, gm))) return rc;
-  // [D | R1 | I] -> S11 = D^-1 R1, D^-1
+  // X R2 -> augD[2]; then [D | R1 | X R2] -> S11 = D^-1 R1 (:347), S12 = D^-1 X R2 (:348)
+  if ((rc = scale_rows(s, pl.s1, n, n, n, nn, pl.X, n, B))) return rc;
+  if ((rc = copy_blocks(s, pl.augD + 2 * nn, s3, pl.s1, nn, nn, B))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
   if ((rc = zgesv(s, n, 2 * n, pl.augD, n, s3, B, pl.piv, pl.st))) return rc;
-  if ((rc = fold_status(s, status, pl.st, B, 1))) return rc;
-  // S12 = D^-1 X R2 -> s2
-  if ((rc = scale_rows(s, pl.s1, n, n, n, nn, pl.X, n, B))) return rc;
-  gm = ZGemm();
-  gm.m = n; gm.n = n; gm.k = n; gm.batch = B;
-  gm.A = pl.augD + 2 * nn; gm.lda = n; gm.sA = s3;
-  gm.B = pl.s1; gm.ldb = n; gm.sB = nn;
-  gm.C = pl.s2; gm.ldc = n; gm.sC = nn;
   (void)zero;
-  return zgemm(s, gm);
+  return fold_status(s, status, pl.st, B, 1);
+}
+
+// Star product with a uniform layer whose S-matrix is BD (2x2-block
+// diagonal): A <- A (x) L, L11 = L22 = Lbd[0], L12 = L21 = Lbd[1]
+// (rcwa.cpp:588-615 with the sparse factors applied in O(n^2)).
+//   [I - L11 A22 | L11 A21 | L12] -> X1 = F^-1 L11 A21, X2 = F^-1 L12
+//   [I - A22 L11 | A21 | A22]     -> Y1 = G^-1 A21,     Y2 = G^-1 A22
+//   S11 = A11 + A12 X1, S12 = A12 X2, S21 = L12 Y1, S22 = L11 + L12 Y2 L12
+int star_product_bd(rcwa_context* ctx, int B, const ModeDims& d, SMat& A, const double2* Lbd,
+                    long long sL, double2*& tmp, double2* augFG, int* piv, uint32_t* st) {
+  cudaStream_t s = ctx->stream;
+  const int n = d.n, N = d.N;
+  const long long nn = (long long)n * n, s3 = 3 * nn;
+  double2* augF = augFG;
+  double2* augG = augFG + (long long)B * s3;
+  const double2* L11 = Lbd;
+  const double2* L12 = Lbd + 4 * N;
+  const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
+  int rc;
+  if ((rc = bd_apply(s, 0, N, n, n, L11, sL, A.p[3], n, A.s[3], augF, n, s3, mone, zero, 1, B))) return rc;
+  if ((rc = bd_apply(s, 0, N, n, n, L11, sL, A.p[2], n, A.s[2], augF + nn, n, s3, one, zero, 0, B))) return rc;
+  if ((rc = bd_dense(s, N, L12, sL, augF + 2 * nn, s3, 0, B))) return rc;
+  if ((rc = bd_apply(s, 1, N, n, n, L11, sL, A.p[3], n, A.s[3], augG, n, s3, mone, zero, 1, B))) return rc;
+  if ((rc = copy_blocks(s, augG + nn, s3, A.p[2], A.s[2], nn, B))) return rc;
+  if ((rc = copy_blocks(s, augG + 2 * nn, s3, A.p[3], A.s[3], nn, B))) return rc;
+  if ((rc = zgesv(s, n, 2 * n, augFG, n, s3, 2 * B, piv, st))) return rc;
+  ZGemm g;
+  g.m = n; g.n = n; g.k = n; g.batch = B;
+  // S11 = A11 + A12 X1
+  g.alpha = one; g.beta = one;
+  g.A = A.p[1]; g.lda = n; g.sA = A.s[1];
+  g.B = augF + nn; g.ldb = n; g.sB = s3;
+  g.C = A.p[0]; g.ldc = n; g.sC = A.s[0];
+  if ((rc = zgemm(s, g))) return rc;
+  // S12 = A12 X2 -> tmp, swapped in below
+  g.beta = zero;
+  g.B = augF + 2 * nn;
+  g.C = tmp; g.sC = nn;
+  if ((rc = zgemm(s, g))) return rc;
+  // S21 = L12 Y1 (A21 was copied into augG)
+  if ((rc = bd_apply(s, 0, N, n, n, L12, sL, augG + nn, n, s3, A.p[2], n, A.s[2], one, zero, 0, B))) return rc;
+  // S22 = L11 + (L12 Y2) L12: L12 Y2 -> augF[0] (F is consumed), then right-apply into A22
+  if ((rc = bd_apply(s, 0, N, n, n, L12, sL, augG + 2 * nn, n, s3, augF, n, s3, one, zero, 0, B))) return rc;
+  if ((rc = bd_apply(s, 1, N, n, n, L12, sL, augF, n, s3, A.p[3], n, A.s[3], one, zero, 0, B))) return rc;
+  if ((rc = bd_dense(s, N, L11, sL, A.p[3], A.s[3], 1, B))) return rc;
+  std::swap(A.p[1], tmp);
+  A.s[1] = nn;
+  return RCWA_OK;
+}
+
+// The two source columns of the global S11 and S21 (main.cpp:166-170; only
+// columns PQ/2 and PQ/2+PQ reach the fields, rcwa.cpp:512-514, 535, 553):
+//   S' = S_ref (x) S_dev, S'' = S' (x) S_trn with S_ref, S_trn in BD form.
+//   G1 = I - R22 D11:  [G1 | R22 D12 | R21 E] -> Z2, y
+//   S'22 = D22 + D21 Z2,  S'21 E = D21 y
+//   F2 = I - T11 S'22: x = F2^-1 T11 S'21 E;  G2 = I - S'22 T11: z = G2^-1 S'21 E
+//   S''21 E = T21 z
+//   F1 = I - D11 R22:  q = F1^-1 (D11 R21 E + D12 x);  S''11 E = R11 E + R12 q
+// Outputs S11E, S21E: n x 2 per source (stride 2n).
+int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, const double2* Rbd,
+                   const double2* Tbd, long long sP, double2* S11E, double2* S21E,
+                   double2* augFG, double2* augWV, double2* augA, double2* s0, double2* s1,
+                   int* piv, uint32_t* st, uint32_t* status) {
+  cudaStream_t s = ctx->stream;
+  const int n = d.n, N = d.N, a = N / 2;
+  const long long nn = (long long)n * n, s6 = 6 * nn, s2 = 2 * nn, c2 = 2LL * n;
+  const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
+  const double2 *R11 = Rbd, *R12 = Rbd + 4 * N, *R21 = Rbd + 8 * N, *R22 = Rbd + 12 * N;
+  const double2 *T11 = Tbd, *T21 = Tbd + 8 * N;
+  int rc;
+  auto gemm = [&](int m, int ncol, double2* C, long long sC, const double2* X, long long sX,
+                  const double2* Y, long long sY, double2 beta) {
+    ZGemm g;
+    g.m = m; g.n = ncol; g.k = n; g.batch = B;
+    g.beta = beta;
+    g.A = X; g.lda = n; g.sA = sX;
+    g.B = Y; g.ldb = n; g.sB = sY;
+    g.C = C; g.ldc = n; g.sC = sC;
+    return zgemm(s, g);
+  };
+  // [G1 | R22 D12 | R21 E] in augFG (stride 6n^2)
+  double2* u = augFG + 2 * nn;
+  if ((rc = bd_apply(s, 0, N, n, n, R22, sP, D.p[0], n, D.s[0], augFG, n, s6, mone, zero, 1, B))) return rc;
+  if ((rc = bd_apply(s, 0, N, n, n, R22, sP, D.p[1], n, D.s[1], augFG + nn, n, s6, one, zero, 0, B))) return rc;
+  if ((rc = bd_cols(s, N, a, R21, sP, u, n, s6, one, zero, B))) return rc;
+  // [F1 | D11 R21 E (+ D12 x later)] in augA (stride 2n^2); F1 = I - D11 R22
+  if ((rc = bd_apply(s, 1, N, n, n, R22, sP, D.p[0], n, D.s[0], augA, n, s2, mone, zero, 1, B))) return rc;
+  if ((rc = gemm(n, 2, augA + nn, s2, D.p[0], D.s[0], u, s6, zero))) return rc;
+  RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 3 * B * sizeof(uint32_t), s));
+  if ((rc = zgesv(s, n, n + 2, augFG, n, s6, B, piv, st))) return rc;
+  if ((rc = fold_status(s, status, st, B, 1))) return rc;
+  // S'22 -> s0, S'21 E -> s1
+  if ((rc = copy_blocks(s, s0, nn, D.p[3], D.s[3], nn, B))) return rc;
+  if ((rc = gemm(n, n, s0, nn, D.p[2], D.s[2], augFG + nn, s6, one))) return rc;
+  if ((rc = gemm(n, 2, s1, nn, D.p[2], D.s[2], u, s6, zero))) return rc;
+  // [F2 | T11 S'21E] (systems 0..B-1) and [G2 | S'21E] (systems B..2B-1) in augWV
+  double2* augG2 = augWV + (long long)B * s2;
+  if ((rc = bd_apply(s, 0, N, n, n, T11, sP, s0, n, nn, augWV, n, s2, mone, zero, 1, B))) return rc;
+  if ((rc = bd_apply(s, 0, N, n, 2, T11, sP, s1, n, nn, augWV + nn, n, s2, one, zero, 0, B))) return rc;
+  if ((rc = bd_apply(s, 1, N, n, n, T11, sP, s0, n, nn, augG2, n, s2, mone, zero, 1, B))) return rc;
+  if ((rc = copy_blocks(s, augG2 + nn, s2, s1, nn, c2, B))) return rc;
+  RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 3 * B * sizeof(uint32_t), s));
+  if ((rc = zgesv(s, n, 2, augWV, n, s2, 2 * B, piv, st))) return rc;
+  if ((rc = fold_status(s, status, st, B, 2))) return rc;
+  // S''21 E = T21 z
+  if ((rc = bd_apply(s, 0, N, n, 2, T21, sP, augG2 + nn, n, s2, S21E, n, c2, one, zero, 0, B))) return rc;
+  // v = D11 R21 E + D12 x, then q = F1^-1 v
+  if ((rc = gemm(n, 2, augA + nn, s2, D.p[1], D.s[1], augWV + nn, s2, one))) return rc;
+  RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 3 * B * sizeof(uint32_t), s));
+  if ((rc = zgesv(s, n, 2, augA, n, s2, B, piv, st))) return rc;
+  if ((rc = fold_status(s, status, st, B, 1))) return rc;
+  // S''11 E = R11 E + R12 q
+  if ((rc = bd_cols(s, N, a, R11, sP, S11E, n, c2, one, zero, B))) return rc;
+  return bd_apply(s, 0, N, n, 2, R12, sP, augA + nn, n, s2, S11E, n, c2, one, one, 0, B);
 }
 
 }  // namespace
@@ -498,25 +607,32 @@ static int sweep_chunk(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_sou
     dev.s[k] = nn;
   }
   double2* tmp = pl.tmp;
+  const long long sL = 8LL * d.N;     // BD uniform layer: S11 (4N) + S12 (4N) per source
   for (int l = 0; l < g->nl; ++l) {
-    SMat lay;
     if (g->uniform[l]) {
-      // S11 -> s0, S12 -> s1 (sparse content, dense storage)
-      if ((rc = fill_zero(s, pl.s0, (size_t)B * nn))) return rc;
-      if ((rc = fill_zero(s, pl.s1, (size_t)B * nn))) return rc;
-      if ((rc = uniform_layer(s, B, d, g->ueps[l], g->umu[l], g->t[l], pl.wv, pl.s0, pl.s1, nn)))
+      if ((rc = uniform_layer(s, B, d, g->ueps[l], g->umu[l], g->t[l], pl.wv, pl.lbd, pl.lbd + 4 * d.N,
+                              sL, 1)))
         return rc;
-      lay.p[0] = pl.s0; lay.s[0] = nn;
-      lay.p[1] = pl.s1; lay.s[1] = nn;
-    } else {
-      if ((rc = patterned_layer(ctx, g, l, pl, status))) return rc;
-      lay.p[0] = pl.augD + nn; lay.s[0] = s3;
-      lay.p[1] = pl.s2; lay.s[1] = nn;
+      if (l == 0) {
+        // S_init (x) S_layer == S_layer exactly (S11 = S22 = 0, S12 = S21 = I)
+        if ((rc = bd_dense(s, d.N, pl.lbd, sL, dev.p[0], nn, 0, B))) return rc;
+        if ((rc = bd_dense(s, d.N, pl.lbd + 4 * d.N, sL, dev.p[1], nn, 0, B))) return rc;
+        if ((rc = bd_dense(s, d.N, pl.lbd + 4 * d.N, sL, dev.p[2], nn, 0, B))) return rc;
+        if ((rc = bd_dense(s, d.N, pl.lbd, sL, dev.p[3], nn, 0, B))) return rc;
+      } else {
+        RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
+        if ((rc = star_product_bd(ctx, B, d, dev, pl.lbd, sL, tmp, pl.augFG, pl.piv, pl.st))) return rc;
+        if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
+      }
+      continue;
     }
-    lay.p[2] = lay.p[1]; lay.s[2] = lay.s[1];   // S21 = S12 (:351)
-    lay.p[3] = lay.p[0]; lay.s[3] = lay.s[0];   // S22 = S11
+    if ((rc = patterned_layer(ctx, g, l, pl, status))) return rc;
+    SMat lay;
+    lay.p[0] = pl.augD + nn; lay.s[0] = s3;      // S11 = D^-1 R1
+    lay.p[1] = pl.augD + 2 * nn; lay.s[1] = s3;  // S12 = D^-1 X R2
+    lay.p[2] = lay.p[1]; lay.s[2] = lay.s[1];    // S21 = S12 (:351)
+    lay.p[3] = lay.p[0]; lay.s[3] = lay.s[0];    // S22 = S11
     if (l == 0) {
-      // S_init (x) S_layer == S_layer exactly (S11 = S22 = 0, S12 = S21 = I)
       for (int k = 0; k < 4; ++k)
         if ((rc = copy_blocks(s, dev.p[k], dev.s[k], lay.p[k], lay.s[k], nn, B))) return rc;
     } else {
@@ -532,31 +648,24 @@ static int sweep_chunk(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_sou
     if ((rc = set_identity(s, dev.p[1], n, n, nn, n, 0, B, make_double2(1, 0)))) return rc;
     if ((rc = set_identity(s, dev.p[2], n, n, nn, n, 0, B, make_double2(1, 0)))) return rc;
   }
+  // S_ref, S_trn in BD form (rcwa.cpp:354-466), then the two source columns of
   // S_ref (x) S_device (x) S_trn (main.cpp:166-170)
-  SMat port;
-  for (int k = 0; k < 4; ++k) {
-    port.p[k] = pl.SP[k];
-    port.s[k] = nn;
-    if ((rc = fill_zero(s, pl.SP[k], (size_t)B * nn))) return rc;
-  }
-  if ((rc = port_smatrix(s, B, d, 0, g->er_ref, g->ur_ref, pl.wv, port.p[0], port.p[1], port.p[2],
-                         port.p[3], nn)))
+  const long long sP = 32LL * d.N;
+  double2* Rbd = pl.pbd;
+  double2* Tbd = pl.pbd + 16 * d.N;
+  if ((rc = port_smatrix(s, B, d, 0, g->er_ref, g->ur_ref, pl.wv, Rbd, Rbd + 4 * d.N, Rbd + 8 * d.N,
+                         Rbd + 12 * d.N, sP, 1)))
     return rc;
-  RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = star_product(ctx, B, n, port, dev, tmp, pl.augFG, pl.piv, pl.st))) return rc;
-  if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
-  // S_trn into the (now free) device blocks
-  for (int k = 0; k < 4; ++k) {
-    if ((rc = fill_zero(s, dev.p[k], (size_t)B * nn))) return rc;
-  }
-  if ((rc = port_smatrix(s, B, d, 1, g->er_trn, g->ur_trn, pl.wv, dev.p[0], dev.p[1], dev.p[2],
-                         dev.p[3], nn)))
+  if ((rc = port_smatrix(s, B, d, 1, g->er_trn, g->ur_trn, pl.wv, Tbd, Tbd + 4 * d.N, Tbd + 8 * d.N,
+                         Tbd + 12 * d.N, sP, 1)))
     return rc;
-  RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = star_product(ctx, B, n, port, dev, tmp, pl.augFG, pl.piv, pl.st))) return rc;
-  if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
+  double2* S11E = pl.s2;
+  double2* S21E = pl.s3;
+  if ((rc = global_columns(ctx, B, d, dev, Rbd, Tbd, sP, S11E, S21E, pl.augFG, pl.augWV, pl.augA,
+                           pl.s0, pl.s1, pl.piv, pl.st, status)))
+    return rc;
   // efficiencies (main.cpp:182-191)
-  return efficiencies(s, B, d, pl.src, g->ur_ref, g->ur_trn, pl.wv, port.p[0], port.p[2], nn, R, T,
+  return efficiencies(s, B, d, pl.src, g->ur_ref, g->ur_trn, pl.wv, S11E, S21E, 2LL * n, 1, R, T,
                       tot, status);
 }
 
@@ -705,7 +814,8 @@ int step_smatrix_layer(rcwa_context* ctx, int N, const double2* erc, const doubl
       (rc = h2d(ctx, pl.wv.V0, V0d, (size_t)4 * N * 16)) || (rc = h2d(ctx, pl.wv.kinc, kinc, sizeof(kinc))))
     return rc;
   if ((rc = patterned_layer(ctx, &g, 0, pl, dst))) return rc;
-  if ((rc = d2h(ctx, S11, pl.augD + nn, nn * 16)) || (rc = d2h(ctx, S12, pl.s2, nn * 16))) return rc;
+  if ((rc = d2h(ctx, S11, pl.augD + nn, nn * 16)) || (rc = d2h(ctx, S12, pl.augD + 2 * nn, nn * 16)))
+    return rc;
   uint32_t hs[2] = {0, 0};
   if ((rc = d2h(ctx, hs, dst, 8))) return rc;
   RCWA_CUDA_TRY(cudaStreamSynchronize(s));
@@ -736,7 +846,7 @@ int step_port(rcwa_context* ctx, int side, int N, double2 er, double2 ur, const 
     return rc;
   for (int k = 0; k < 4; ++k)
     if ((rc = fill_zero(s, dS[k], nn))) return rc;
-  if ((rc = port_smatrix(s, 1, d, side, er, ur, w, dS[0], dS[1], dS[2], dS[3], (long long)nn))) return rc;
+  if ((rc = port_smatrix(s, 1, d, side, er, ur, w, dS[0], dS[1], dS[2], dS[3], (long long)nn, 0))) return rc;
   for (int k = 0; k < 4; ++k)
     if ((rc = d2h(ctx, S[k], dS[k], nn * 16))) return rc;
   RCWA_CUDA_TRY(cudaStreamSynchronize(s));
@@ -804,7 +914,7 @@ int step_efficiencies(rcwa_context* ctx, const rcwa_source* src, const rcwa_para
     return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 4, ctx->stream));
   if ((rc = efficiencies(ctx->stream, 1, d, ds, c2(p->ur_ref), c2(p->ur_trn), w, dS11, dS21,
-                         (long long)nn, dR, dT, dtot, st)))
+                         (long long)nn, 0, dR, dT, dtot, st)))
     return rc;
   double htot[2];
   uint32_t hst = 0;
