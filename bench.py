@@ -284,6 +284,7 @@ def main():
     dms, dn, dfl = fam[dom]
     achieved = (dfl / dn) / (dms / dn / 1e3) / 1e12 if dn and dfl else None
     shares = {k: round(v[0] / max(1e-9, sum(x[0] for x in fam.values())), 4) for k, v in fam.items()}
+    fam_tflops = {k: (round(v[2] / (v[0] / 1e3) / 1e12, 3) if v[0] and v[2] else None) for k, v in fam.items()}
 
     solves = B * args.steps * world
     value = solves / (dev_ms / 1e3)
@@ -327,7 +328,7 @@ def main():
                      "traffic": None,
                      "peak_source": "cuBLAS ZGEMM 4096^3 (complex128) measured in this run",
                      "launches": dn, "avg_launch_ms": dms / dn if dn else None,
-                     "family_time_share": shares},
+                     "family_time_share": shares, "family_tflops": fam_tflops},
         "cpu_baseline": cpu,
         "clocks": clocks,
     }
