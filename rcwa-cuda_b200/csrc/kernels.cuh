@@ -36,6 +36,7 @@ struct ZGemm {
   const double2* dr = nullptr;  // optional right (column) scaling, stride sdr per batch
   long long sdr = 0;
   int batch = 1;
+  int opA = 0, opB = 0;         // 1 = use the conjugate transpose of the stored operand
 };
 int zgemm(cudaStream_t s, const ZGemm& g);
 
@@ -43,6 +44,13 @@ int zgemm(cudaStream_t s, const ZGemm& g);
 int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch,
           int* piv, uint32_t* status);
 
+// Blocked Hessenberg reduction of packed A (zero below the subdiagonal on
+// return) and Z = Q; V is an n x n scratch per matrix, ws hess_ws_bytes().
+size_t hess_ws_bytes(int n, int batch);
+int hess_blocked(cudaStream_t s, int n, int batch, double2* A, double2* Z, double2* V, void* ws);
+// Complex Schur form of upper Hessenberg H (in place) with Z <- Z * Schur vectors.
+int schur_launch(cudaStream_t s, double2* H, int ld, long long sH, int n, double2* Z, double2* lam,
+                 long long slam, uint32_t* status, int batch);
 // Eigen-decomposition of packed n x n matrices (destroyed).
 size_t zeig_workspace_bytes(int n, int batch);
 int zeig(cudaStream_t s, int n, int batch, double2* A, int ld, long long sA, double2* W,

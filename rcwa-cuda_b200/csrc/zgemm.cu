@@ -34,6 +34,8 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+// OPA / OPB: 0 = the operand as stored, 1 = its conjugate transpose.
+template <int OPA, int OPB>
 __global__ void __launch_bounds__(NT, 2)
 zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, int lda,
              long long sA, const double2* __restrict__ B, int ldb, long long sB, double2 beta,
@@ -61,18 +63,22 @@ zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, 
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       int e = tid + h * NT;
-      // A tile: 64 rows x 8 k
-      int r = e & 63, kk = e >> 6;
-      int gr = m0 + r, gk = k0 + kk;
-      bool pa = (gr < m) && (gk < k);
-      const double2* srcA = pa ? (A + (long long)gk * lda + gr) : A;
-      cp_async16(&As[buf][kk][r], srcA, pa);
+      // A tile: 64 rows x 8 k (consecutive threads walk the contiguous index)
+      {
+        const int r = OPA ? (e >> 3) : (e & 63), kk = OPA ? (e & 7) : (e >> 6);
+        const int gr = m0 + r, gk = k0 + kk;
+        const bool pa = (gr < m) && (gk < k);
+        const double2* srcA = pa ? (OPA ? A + (long long)gr * lda + gk : A + (long long)gk * lda + gr) : A;
+        cp_async16(&As[buf][kk][r], srcA, pa);
+      }
       // B tile: 8 k x 64 cols
-      int kb = e & 7, c = e >> 3;
-      int gk2 = k0 + kb, gc = n0 + c;
-      bool pb = (gk2 < k) && (gc < n);
-      const double2* srcB = pb ? (B + (long long)gc * ldb + gk2) : B;
-      cp_async16(&Bs[buf][kb][c], srcB, pb);
+      {
+        const int kb = OPB ? (e >> 6) : (e & 7), c = OPB ? (e & 63) : (e >> 3);
+        const int gk2 = k0 + kb, gc = n0 + c;
+        const bool pb = (gk2 < k) && (gc < n);
+        const double2* srcB = pb ? (OPB ? B + (long long)gk2 * ldb + gc : B + (long long)gc * ldb + gk2) : B;
+        cp_async16(&Bs[buf][kb][c], srcB, pb);
+      }
     }
     cp_async_commit();
   };
@@ -92,9 +98,15 @@ zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, 
     for (int kk = 0; kk < BK; ++kk) {
       double2 a[4], bb[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][tx + 16 * i];
+      for (int i = 0; i < 4; ++i) {
+        a[i] = As[buf][kk][tx + 16 * i];
+        if (OPA) a[i].y = -a[i].y;
+      }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bb[j] = Bs[buf][kk][ty + 16 * j];
+      for (int j = 0; j < 4; ++j) {
+        bb[j] = Bs[buf][kk][ty + 16 * j];
+        if (OPB) bb[j].y = -bb[j].y;
+      }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -127,14 +139,18 @@ zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, 
 
 int zgemm(cudaStream_t s, const ZGemm& g) {
   if (g.m <= 0 || g.n <= 0 || g.batch <= 0) return RCWA_OK;
-  if (g.k <= 0) {
-    // C = beta*C: reuse the kernel with k = 0 (acc stays 0).
-  }
+  // k <= 0 gives C = beta*C (the accumulators stay 0)
   dim3 grid(cdiv_up(g.n, BN), cdiv_up(g.m, BM), g.batch);
   void* tok = prof_begin(s);
-  zgemm_kernel<<<grid, NT, 0, s>>>(g.m, g.n, g.k < 0 ? 0 : g.k, g.alpha, g.A, g.lda, g.sA, g.B,
-                                   g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, g.dr,
-                                   g.sdr);
+  const int kk = g.k < 0 ? 0 : g.k;
+#define RCWA_ZGEMM_ARGS                                                                          \
+  g.m, g.n, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
+      g.dr, g.sdr
+  if (g.opA == 0 && g.opB == 0) zgemm_kernel<0, 0><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
+  else if (g.opA == 1 && g.opB == 0) zgemm_kernel<1, 0><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
+  else if (g.opA == 0 && g.opB == 1) zgemm_kernel<0, 1><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
+  else zgemm_kernel<1, 1><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
+#undef RCWA_ZGEMM_ARGS
   prof_end(s, tok, "zgemm");
   if (tok) {
     // algorithmic flops of this launch, for the roofline (8 m n k per matrix)
