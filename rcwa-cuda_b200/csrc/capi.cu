@@ -427,7 +427,7 @@ int rcwa_lu_solve(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_comp
 int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_complex* A,
               const rcwa_complex* B, rcwa_complex* C, int precision) {
   CHECK_ARG(ctx && A && B && C && m > 0 && n > 0 && k > 0 && batch > 0, "bad argument");
-  CHECK_ARG(precision == RCWA_PREC_FP64, "precision mode not available in this build");
+  CHECK_ARG(precision == RCWA_PREC_FP64 || precision == RCWA_PREC_MIXED, "unknown precision mode");
   RCWA_CUDA_TRY(cudaSetDevice(ctx->device));
   const size_t na = (size_t)m * k, nb = (size_t)k * n, nc = (size_t)m * n;
   int rc = ctx_reserve(ctx, (na + nb + nc) * batch * 16 + 1024);
@@ -443,9 +443,18 @@ int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_comp
   g.A = dA; g.lda = m; g.sA = (long long)na;
   g.B = dB; g.ldb = k; g.sB = (long long)nb;
   g.C = dC; g.ldc = m; g.sC = (long long)nc;
+  g.tc = precision == RCWA_PREC_MIXED ? 1 : 0;
+  int* terr = g.tc ? tc_error_flag() : nullptr;
+  if (terr) RCWA_CUDA_TRY(cudaMemsetAsync(terr, 0, sizeof(int), s));
   if ((rc = zgemm(s, g))) return rc;
   RCWA_CUDA_TRY(cudaMemcpyAsync(C, dC, nc * batch * 16, cudaMemcpyDeviceToHost, s));
+  int herr = 0;
+  if (terr) RCWA_CUDA_TRY(cudaMemcpyAsync(&herr, terr, sizeof(int), cudaMemcpyDeviceToHost, s));
   RCWA_CUDA_TRY(cudaStreamSynchronize(s));
+  if (herr) {
+    set_last_error("tensor-core GEMM: a bounded wait on the MMA barrier expired");
+    return RCWA_ERR_CUDA;
+  }
   return RCWA_OK;
 }
 

@@ -37,8 +37,12 @@ struct ZGemm {
   long long sdr = 0;
   int batch = 1;
   int opA = 0, opB = 0;         // 1 = use the conjugate transpose of the stored operand
+  int tc = 0;                   // 1 = split-TF32 on tcgen05 (mixed-precision mode)
 };
 int zgemm(cudaStream_t s, const ZGemm& g);
+// split-TF32 tcgen05 GEMM (ztc.cu); *err is set when a bounded wait expires
+int zgemm_tc(cudaStream_t s, const ZGemm& g, int* err);
+int* tc_error_flag();   // device flag of the current device (set-up once per device)
 
 // X = A^-1 B on the augmented [A | B] (n x (n+nrhs), column-major, ld >= n).
 int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch,

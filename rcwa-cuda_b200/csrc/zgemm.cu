@@ -277,6 +277,14 @@ int gemm_impl() {
 
 int zgemm(cudaStream_t s, const ZGemm& g) {
   if (g.m <= 0 || g.n <= 0 || g.batch <= 0) return RCWA_OK;
+  if (g.tc && !g.opA && !g.opB) {
+    int* err = tc_error_flag();
+    if (!err) {
+      set_last_error("tensor-core GEMM: device flag unavailable");
+      return RCWA_ERR_CUDA;
+    }
+    return zgemm_tc(s, g, err);
+  }
   // k <= 0 gives C = beta*C (the accumulators stay 0)
   dim3 grid(cdiv_up(g.n, BN), cdiv_up(g.m, BM), g.batch);
   void* tok = prof_begin(s);

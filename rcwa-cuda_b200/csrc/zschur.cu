@@ -42,12 +42,29 @@ constexpr int MS_MIN = 3 * NS;
 constexpr int WINMAX = MWIN > SWIN ? MWIN : SWIN;
 static_assert(WINMAX <= 32, "one lane per window column");
 
+// Optional per-launch counters of matrix 0 (compile with -DRCWA_SCHUR_STATS):
+// [0] multishift sweeps [1] single sweeps [2] cycles in multishift sweeps
+// [3] cycles in single sweeps [4] cycles computing shifts [5] exceptional
+// shifts [6] total cycles [7] deflation scans
+#ifdef RCWA_SCHUR_STATS
+__device__ unsigned long long g_schur_stats[16];
+#define SCHUR_STAT(i, v) \
+  do { if (blockIdx.x == 0 && threadIdx.x == 0) g_schur_stats[i] += (unsigned long long)(v); } while (0)
+#define SCHUR_STAT_T(t, i, v) \
+  do { if (blockIdx.x == 0 && threadIdx.x == (t)) g_schur_stats[i] += (unsigned long long)(v); } while (0)
+#else
+#define SCHUR_STAT(i, v) do { } while (0)
+#define SCHUR_STAT_T(t, i, v) do { } while (0)
+#endif
+
 struct Smem {
   double2 Hw[WINMAX][WINMAX + 1];  // window, Hw[col][row]
-  double2 rtau[MW][NS];
-  double2 rv[MW][NS];
+  // multishift reflector log of a chunk, double buffered (chase of chunk c+1
+  // runs while chunk c is applied): tau, v2, active flag
+  double2 rtau[2][MW][NS];
+  double2 rv[2][MW][NS];
+  int ract[2][MW][NS];
   double rbeta[MW][NS];
-  int ract[MW][NS];
   double2 stau[SW];
   double2 sv[SW];
   double2 Hs[NS][NS + 1];          // trailing block for the shifts, Hs[col][row]
@@ -218,114 +235,247 @@ __device__ void single_sweep(Smem& sm, double2* H, double2* Z, int ld, int n, in
 }
 
 // ---- multishift sweep over [l, i] with NS bulges (shifts in sm.shifts) --------
-// Bulge b enters at step 2b; at step t it sits at k = l + t - 2b.
-__device__ void multi_sweep(Smem& sm, double2* H, double2* Z, int ld, int n, int l, int i) {
+// Bulge b enters at step 2b; at step t it sits at k = l + t - 2b.  Chunk c
+// covers steps [c*MW, c*MW + MW); its reflectors touch rows/columns
+// [kbase, kbase + NR) with kbase = l + c*MW - 2(NS-1).
+
+// Chase of one chunk by one warp inside the shared window; logs to buffer buf.
+// At step t bulge b acts on window rows/columns (kk_b, kk_b + 1) with
+// kk_b = base + 2 (NS - 1 - b): the NS pairs tile [base, base + 2 NS).  The
+// left applications run with one lane per window column, the right ones with
+// one lane per window row; each lane holds its 2 NS entries in registers and
+// applies all bulges branch-free (a reflector that does not reach the lane's
+// column or row, or belongs to an inactive bulge, gets tau = 0: the identity).
+__device__ void ms_chase(Smem& sm, int buf, int l, int i, int T, int t0, int j0, int nw, int lane) {
+#pragma unroll 1
+  for (int s = 0; s < MW; ++s) {
+    const int t = t0 + s;
+    if (lane < NS) {
+      const int b = lane, k = l + t - 2 * b;
+      const bool act = (t < T) && k >= l && k <= i - 1;
+      double beta = 0.0;
+      double2 tau = cmk(0.0, 0.0), v2 = cmk(0.0, 0.0);
+      if (act) {
+        const int kk = k - j0;
+        double2 alpha, x;
+        if (k == l) {
+          alpha = csub(sm.Hw[kk][kk], sm.shifts[b]);
+          x = sm.Hw[kk][kk + 1];
+        } else {
+          alpha = sm.Hw[kk - 1][kk];
+          x = sm.Hw[kk - 1][kk + 1];
+        }
+        larfg2(alpha, x, beta, tau, v2);
+      }
+      sm.rtau[buf][s][b] = tau;
+      sm.rv[buf][s][b] = v2;
+      sm.rbeta[s][b] = beta;
+      sm.ract[buf][s][b] = act ? 1 : 0;
+    }
+    __syncwarp();
+    const int base = l + t - j0 - 2 * (NS - 1);
+    double2 x[2 * NS];
+    {  // left: lane = window column c
+      const int c = lane;
+#pragma unroll
+      for (int r = 0; r < 2 * NS; ++r) {
+        const int row = base + r;
+        x[r] = (c < nw && row >= 0 && row < nw) ? sm.Hw[c][row] : cmk(0.0, 0.0);
+      }
+#pragma unroll
+      for (int b = 0; b < NS; ++b) {
+        const int p = 2 * (NS - 1 - b), kk = base + p;
+        const bool act = lds1(&sm.ract[buf][s][b]) != 0;
+        const double2 tau = (act && c >= kk) ? lds2(&sm.rtau[buf][s][b]) : cmk(0.0, 0.0);
+        refl_left(x[p], x[p + 1], tau, lds2(&sm.rv[buf][s][b]));
+        if (act && c == kk - 1 && kk + j0 > l) {
+          x[p] = cmk(sm.rbeta[s][b], 0.0);
+          x[p + 1] = cmk(0.0, 0.0);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 2 * NS; ++r) {
+        const int row = base + r;
+        if (c < nw && row >= 0 && row < nw) sm.Hw[c][row] = x[r];
+      }
+    }
+    __syncwarp();
+    {  // right: lane = window row r
+      const int r = lane;
+#pragma unroll
+      for (int q = 0; q < 2 * NS; ++q) {
+        const int col = base + q;
+        x[q] = (r < nw && col >= 0 && col < nw) ? sm.Hw[col][r] : cmk(0.0, 0.0);
+      }
+#pragma unroll
+      for (int b = 0; b < NS; ++b) {
+        const int p = 2 * (NS - 1 - b), kk = base + p;
+        const bool act = lds1(&sm.ract[buf][s][b]) != 0;
+        const double2 tau =
+            (act && r <= min(kk + j0 + 2, i) - j0) ? lds2(&sm.rtau[buf][s][b]) : cmk(0.0, 0.0);
+        refl_right(x[p], x[p + 1], tau, lds2(&sm.rv[buf][s][b]));
+      }
+#pragma unroll
+      for (int q = 0; q < 2 * NS; ++q) {
+        const int col = base + q;
+        if (r < nw && col >= 0 && col < nw) sm.Hw[col][r] = x[q];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Applies the logged reflectors of one chunk (buffer buf) to one item: the
+// NR entries p[r * stride], r in [0, NR) (rows kbase + r of a column, or
+// columns kbase + r of a row); entries outside [rlo, rhi] are not read (zero)
+// nor written.  Step t's reflector of bulge b acts on entries
+// (t + 2 (NS-1-b), +1), so after step t entry t is final: the register
+// window y slides down by two entries every two steps (y[j] = x[t + j]) and
+// the rotations use fixed register indices inside a rolled loop, which keeps
+// the hot loop small enough for the instruction cache.  Inactive reflectors
+// are logged as tau = v2 = 0, the identity, so no rotation is branched.
+template <bool LEFT>
+__device__ __forceinline__ void ms_rotate_item(const Smem& sm, int buf, double2* p, long long stride,
+                                               int rlo, int rhi) {
+  double2 y[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) y[r] = (r >= rlo && r <= rhi) ? p[r * stride] : cmk(0.0, 0.0);
+#pragma unroll 1
+  for (int t = 0; t < MW; t += 2) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int b = 0; b < NS; ++b) {
+        const int q = h + 2 * (NS - 1 - b);
+        const double2 tau = lds2(&sm.rtau[buf][t + h][b]), v2 = lds2(&sm.rv[buf][t + h][b]);
+        if (LEFT)
+          refl_left(y[q], y[q + 1], tau, v2);
+        else
+          refl_right(y[q], y[q + 1], tau, v2);
+      }
+    if (t >= rlo && t <= rhi) p[t * stride] = y[0];
+    if (t + 1 >= rlo && t + 1 <= rhi) p[(t + 1) * stride] = y[1];
+#pragma unroll
+    for (int j = 0; j + 2 < NR; ++j) y[j] = y[j + 2];
+  }
+#pragma unroll
+  for (int r = 0; r + MW < NR; ++r)
+    if (r + MW >= rlo && r + MW <= rhi) p[(r + MW) * stride] = y[r];
+}
+
+// Left application to H columns [c0, c1), rows [lo, hi], by warp group
+// member g of ng.  A column segment is contiguous in memory, so the warp
+// moves 32 columns at a time through its staging tile st[32][NR] with
+// coalesced loads and stores (one lane per row), and each lane rotates one
+// column in registers.
+__device__ __noinline__ void ms_apply_cols(const Smem& sm, int buf, double2* H, int ld, int kbase, int lo,
+                                           int hi, int c0, int c1, double2* st, int g, int ng, int lane) {
+  const int row = kbase + lane;
+  const bool rok = lane < NR && row >= lo && row <= hi;
+  for (int t0 = c0 + 32 * g; t0 < c1; t0 += 32 * ng) {
+    const int ncol = min(32, c1 - t0);
+    const double2* src = H + (long long)t0 * ld + row;
+    // all loads of a batch are issued before any staging store (the stores
+    // could alias the global source as far as the compiler knows)
+#pragma unroll
+    for (int cb = 0; cb < 32; cb += 16) {
+      double2 v[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u)
+        v[u] = (cb + u < ncol && rok) ? src[(long long)(cb + u) * ld] : cmk(0.0, 0.0);
+#pragma unroll
+      for (int u = 0; u < 16; ++u)
+        if (cb + u < ncol && lane < NR) st[(cb + u) * NR + lane] = v[u];
+    }
+    __syncwarp();
+    if (lane < ncol) ms_rotate_item<true>(sm, buf, st + lane * NR, 1, 0, NR - 1);
+    __syncwarp();
+    double2* dst = H + (long long)t0 * ld + row;
+#pragma unroll
+    for (int cb = 0; cb < 32; cb += 16) {
+      double2 v[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) v[u] = st[(cb + u) * NR + (lane < NR ? lane : 0)];
+#pragma unroll
+      for (int u = 0; u < 16; ++u)
+        if (cb + u < ncol && rok) dst[(long long)(cb + u) * ld] = v[u];
+    }
+    __syncwarp();
+  }
+}
+
+// Right application to H rows [0, nB) and all n rows of Z at columns
+// [lo, hi]; one row per thread (lanes take consecutive rows: coalesced).
+__device__ __noinline__ void ms_apply_rows(const Smem& sm, int buf, double2* H, double2* Z, int ld, int n,
+                                           int kbase, int lo, int hi, int nB, int first, int stride) {
+  for (int it = first; it < nB + n; it += stride) {
+    double2* p = (it < nB) ? H + it : Z + (it - nB);
+    ms_rotate_item<false>(sm, buf, p + (long long)kbase * ld, ld, lo - kbase, hi - kbase);
+  }
+}
+
+// Pipelined sweep: while warp 0 brings window c+1 up to date (chunk c's
+// reflectors on its new columns), chases it and writes it back, warps 1..
+// apply chunk c's reflectors to the remaining far columns, the rows above
+// window c and Z.  Window c+1 never overlaps what warps 1.. touch in that
+// iteration: their columns lie right of window c+1, their rows above
+// window c.
+__device__ void multi_sweep(Smem& sm, double2* stage, double2* H, double2* Z, int ld, int n, int l, int i) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int T = (i - l) + 2 * (NS - 1);
-  for (int t0 = 0; t0 < T; t0 += MW) {
-    const int kbase = l + t0 - 2 * (NS - 1);   // register row 0 of this chunk
-    const int j0 = max(l, kbase - 1), j1 = min(i, kbase + NR + 1);
-    const int nw = j1 - j0 + 1;
-    load_window(sm, H, ld, j0, nw);
+  const int C = (T + MW - 1) / MW;
+  auto geom = [&](int c, int& kbase, int& j0, int& j1) {
+    kbase = l + c * MW - 2 * (NS - 1);
+    j0 = max(l, kbase - 1);
+    j1 = min(i, kbase + NR + 1);
+  };
+  {
+    int kb, j0, j1;
+    geom(0, kb, j0, j1);
+    load_window(sm, H, ld, j0, j1 - j0 + 1);
     __syncthreads();
+    if (wid == 0) ms_chase(sm, 0, l, i, T, 0, j0, j1 - j0 + 1, lane);
+    __syncthreads();
+    store_window(sm, H, ld, j0, j1 - j0 + 1);
+    __syncthreads();
+  }
+  for (int c = 0; c < C; ++c) {
+    const int buf = c & 1;
+    int kb, j0, j1;
+    geom(c, kb, j0, j1);
+    const int lo = max(l, kb), hi = min(i, kb + NR - 1);
+    const bool next = c + 1 < C;
+    int kbn = 0, j0n = 0, j1n = j1;
+    if (next) geom(c + 1, kbn, j0n, j1n);
+    const long long cc0 = clock64();
     if (wid == 0) {
-      for (int s = 0; s < MW; ++s) {
-        const int t = t0 + s;
-        if (lane < NS) {
-          const int b = lane, k = l + t - 2 * b;
-          const bool act = (t < T) && k >= l && k <= i - 1;
-          double beta = 0.0;
-          double2 tau = cmk(0.0, 0.0), v2 = cmk(0.0, 0.0);
-          if (act) {
-            const int kk = k - j0;
-            double2 alpha, x;
-            if (k == l) {
-              alpha = csub(sm.Hw[kk][kk], sm.shifts[b]);
-              x = sm.Hw[kk][kk + 1];
-            } else {
-              alpha = sm.Hw[kk - 1][kk];
-              x = sm.Hw[kk - 1][kk + 1];
-            }
-            larfg2(alpha, x, beta, tau, v2);
-          }
-          sm.rtau[s][b] = tau;
-          sm.rv[s][b] = v2;
-          sm.rbeta[s][b] = beta;
-          sm.ract[s][b] = act ? 1 : 0;
+      if (next) {
+        // window c+1's new columns (j1, j1n] still lack chunk c's reflectors
+        ms_apply_cols(sm, buf, H, ld, kb, lo, hi, j1 + 1, j1n + 1, stage, 0, 1, lane);
+        __syncwarp();
+        SCHUR_STAT_T(0, 9, clock64() - cc0);
+        const int nw = j1n - j0n + 1;
+        for (int e = lane; e < nw * nw; e += 32) {
+          const int r = e % nw, cc = e / nw;
+          sm.Hw[cc][r] = H[(long long)(j0n + cc) * ld + j0n + r];
         }
         __syncwarp();
-        // all left applications (rows of distinct bulges are disjoint)
-        for (int it = lane; it < NS * nw; it += 32) {
-          const int b = it / nw, c = it - b * nw;
-          if (!sm.ract[s][b]) continue;
-          const int k = l + t - 2 * b, kk = k - j0;
-          if (c >= kk) {
-            refl_left(sm.Hw[c][kk], sm.Hw[c][kk + 1], sm.rtau[s][b], sm.rv[s][b]);
-          } else if (c == kk - 1 && k > l) {
-            sm.Hw[c][kk] = cmk(sm.rbeta[s][b], 0.0);
-            sm.Hw[c][kk + 1] = cmk(0.0, 0.0);
-          }
-        }
-        __syncwarp();
-        // all right applications (columns of distinct bulges are disjoint)
-        for (int it = lane; it < NS * nw; it += 32) {
-          const int b = it / nw, r = it - b * nw;
-          if (!sm.ract[s][b]) continue;
-          const int k = l + t - 2 * b, kk = k - j0;
-          if (r <= min(k + 2, i) - j0) refl_right(sm.Hw[kk][r], sm.Hw[kk + 1][r], sm.rtau[s][b], sm.rv[s][b]);
-        }
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    store_window(sm, H, ld, j0, nw);
-    // deferred: rows [kbase, kbase+NR) of the columns right of the window,
-    // columns [kbase, kbase+NR) of the rows above it and of Z
-    const int lo = max(l, kbase), hi = min(i, kbase + NR - 1);
-    const int nA = n - 1 - j1, nB = j0, nC = n;
-    for (int it = tid; it < nA + nB + nC; it += NT) {
-      double2 x[NR];
-      if (it < nA) {
-        double2* col = H + (long long)(j1 + 1 + it) * ld;
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-          const int row = kbase + r;
-          x[r] = (row >= lo && row <= hi) ? col[row] : cmk(0.0, 0.0);
-        }
-#pragma unroll
-        for (int s = 0; s < MW; ++s)
-#pragma unroll
-          for (int b = 0; b < NS; ++b)
-            if (lds1(&sm.ract[s][b]))
-              refl_left(x[s + 2 * (NS - 1 - b)], x[s + 2 * (NS - 1 - b) + 1], lds2(&sm.rtau[s][b]),
-                        lds2(&sm.rv[s][b]));
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-          const int row = kbase + r;
-          if (row >= lo && row <= hi) col[row] = x[r];
-        }
-      } else {
-        double2* p = (it < nA + nB) ? H + (it - nA) : Z + (it - nA - nB);
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-          const int c = kbase + r;
-          x[r] = (c >= lo && c <= hi) ? p[(long long)c * ld] : cmk(0.0, 0.0);
-        }
-#pragma unroll
-        for (int s = 0; s < MW; ++s)
-#pragma unroll
-          for (int b = 0; b < NS; ++b)
-            if (lds1(&sm.ract[s][b]))
-              refl_right(x[s + 2 * (NS - 1 - b)], x[s + 2 * (NS - 1 - b) + 1], lds2(&sm.rtau[s][b]),
-                         lds2(&sm.rv[s][b]));
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-          const int c = kbase + r;
-          if (c >= lo && c <= hi) p[(long long)c * ld] = x[r];
+        ms_chase(sm, buf ^ 1, l, i, T, (c + 1) * MW, j0n, nw, lane);
+        for (int e = lane; e < nw * nw; e += 32) {
+          const int r = e % nw, cc = e / nw;
+          H[(long long)(j0n + cc) * ld + j0n + r] = sm.Hw[cc][r];
         }
       }
+      SCHUR_STAT_T(0, 8, clock64() - cc0);
+    } else {
+      ms_apply_cols(sm, buf, H, ld, kb, lo, hi, j1n + 1, n, stage + (size_t)wid * 32 * NR, wid - 1,
+                    NT / 32 - 1, lane);
+      ms_apply_rows(sm, buf, H, Z, ld, n, kb, lo, hi, j0, tid - 32, NT - 32);
+      SCHUR_STAT_T(32, 10, clock64() - cc0);
     }
     __syncthreads();
+    SCHUR_STAT(11, clock64() - cc0);
+    SCHUR_STAT(12, 1);
   }
 }
 
@@ -334,6 +484,7 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
              double2* __restrict__ lamg, long long slam, uint32_t* __restrict__ status,
              int max_sweeps_per_n) {
   __shared__ Smem sm;
+  extern __shared__ double2 stage[];   // [NT/32][32][NR] column staging tiles
   const int b = blockIdx.x;
   double2* H = Hg + (long long)b * stride;
   double2* Z = Zg + (long long)b * stride;
@@ -357,6 +508,7 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
 
   const int itmax = 30 * (n > 10 ? n : 10);
   const long long sweep_cap = (long long)max_sweeps_per_n * (n > 10 ? n : 10);
+  const long long c_start = clock64();
   long long total = 0;
   bool failed = false;
   int i = n - 1;
@@ -365,6 +517,7 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
     bool conv = false;
     for (int its = 0; its <= itmax; ++its) {
       // deflation: largest k in (l, i] with a negligible H[k, k-1]
+      SCHUR_STAT(7, 1);
       int cand = l;
       for (int k = l + 1 + tid; k <= i; k += NT)
         if (k > cand && negligible(H, ld, n, k, ulp, smlnum)) cand = k;
@@ -398,7 +551,9 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
           }
           __syncthreads();
           if (wid == 0) {
+            const long long c3 = clock64();
             const bool ok = small_eig(sm, NS, lane);
+            SCHUR_STAT(4, clock64() - c3);
             if (lane == 0) sm.flag = ok ? 0 : 1;
           }
           __syncthreads();
@@ -408,13 +563,17 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
           exc = sm.flag != 0;
         }
         if (exc) {
+          SCHUR_STAT(5, 1);
           if (tid < NS) {   // zlaqr0: H(k,k) + 0.75 |H(k,k-1)| down the trailing diagonal
             const int k = i - tid;
             sm.shifts[tid] = cadd(H[(long long)k * ld + k], cmk(0.75 * cabs1(H[(long long)(k - 1) * ld + k]), 0.0));
           }
           __syncthreads();
         }
-        multi_sweep(sm, H, Z, ld, n, l, i);
+        const long long c1 = clock64();
+        multi_sweep(sm, stage, H, Z, ld, n, l, i);
+        SCHUR_STAT(0, 1);
+        SCHUR_STAT(2, clock64() - c1);
       } else {
         if (tid == 0) {
           double2 t;
@@ -431,7 +590,10 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
         }
         __syncthreads();
         if (sm.flag) break;
+        const long long c2 = clock64();
         single_sweep(sm, H, Z, ld, n, l, i, sm.shift);
+        SCHUR_STAT(1, 1);
+        SCHUR_STAT(3, clock64() - c2);
       }
     }
     if (!conv) {
@@ -446,14 +608,37 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
     if (tid == 0) atomicOr(status + b, (unsigned)ST_EIG_NOCONV);
     for (int r = tid; r <= i; r += NT) lam[r] = cmk(nan(""), nan(""));
   }
+  SCHUR_STAT(6, clock64() - c_start);
+  (void)c_start;
 }
 
 }  // namespace
 
+#ifdef RCWA_SCHUR_STATS
+extern "C" int rcwa_debug_schur_stats(unsigned long long* out, int reset) {
+  cudaDeviceSynchronize();
+  cudaMemcpyFromSymbol(out, g_schur_stats, sizeof(unsigned long long) * 16);
+  if (reset) {
+    unsigned long long z[16] = {};
+    cudaMemcpyToSymbol(g_schur_stats, z, sizeof(z));
+  }
+  return 0;
+}
+#endif
+
 int schur_launch(cudaStream_t s, double2* H, int ld, long long sH, int n, double2* Z, double2* lam,
                  long long slam, uint32_t* status, int batch) {
   void* tok = prof_begin(s);
-  schur_kernel<<<batch, NT, 0, s>>>(H, ld, sH, n, Z, lam, slam, status, 100);
+  constexpr size_t stage_bytes = sizeof(double2) * (NT / 32) * 32 * NR;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_set[dev]) {
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(schur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)stage_bytes));
+    attr_set[dev] = true;
+  }
+  schur_kernel<<<batch, NT, stage_bytes, s>>>(H, ld, sH, n, Z, lam, slam, status, 100);
   prof_end(s, tok, "schur");
   // work convention: eig with vectors = 100 n^3 real flops per complex matrix,
   // of which Hessenberg (40/3), Q (16/3), triangular vectors (4/3) and the
