@@ -44,7 +44,7 @@ UNIT = "solves/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n-lambda", type=int, default=201)
@@ -187,7 +187,7 @@ def main():
         g = ctx.geometry_create(st, par, er_d.data_ptr(), ur_d.data_ptr(), t_d.data_ptr())
         ctx.solve_sweep_device(g, srcs, L.PREC_FP64, R_d.data_ptr(), T_d.data_ptr(), tot_d.data_ptr(),
                                st_d.data_ptr())
-        ctx.geometry_destroy(g)   # synchronises the stream
+        ctx.geometry_destroy(g)   # stream-ordered release, no host sync
 
     def barrier():
         if world > 1:
@@ -236,7 +236,7 @@ def main():
     prof_step_ms = pa.elapsed_time(pb)
     fam = {}
     # disjoint families ("hess" brackets the whole blocked reduction incl. its GEMMs)
-    for name in ("zgemm", "hess_panel", "schur", "trevc", "lu_panel"):
+    for name in ("zgemm", "zgemm_rank", "hess_panel", "schur", "trevc", "lu_panel"):
         fam[name] = L.profile_query(name)
     hess_all = L.profile_query("hess")
     L.profile_reset()
@@ -333,6 +333,7 @@ def main():
                    "anomalies": int(((stat_h & L.STATUS_WOOD_ANOMALY) != 0).sum()),
                    "step_ms_p50": statistics.median(per_step),
                    "step_ms_p99": float(np.percentile(per_step, 99)),
+                   "step_ms": [round(x, 1) for x in per_step],
                    "max_abs_dR_dT_vs_oracle": err},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),

@@ -121,9 +121,13 @@ int rcwa_solve_sweep(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_sour
 
 /* Geometry handle: the per-layer convolution matrices (main.cpp:125-138,
  * rcwa.cpp:6-82) built once on the device and reused by every source.  With
- * stack_on_device != 0 the stack's er/ur/t pointers are device pointers. */
+ * stack_on_device != 0 the stack's er/ur/t pointers are device pointers.
+ * Its device memory comes from the stream-ordered pool on the context's
+ * stream: use a geometry only with the context that created it. */
 int rcwa_geometry_create(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_params* params,
                          int stack_on_device, rcwa_geometry** out);
+/* Releases the geometry in stream order on its context's stream (work already
+ * enqueued that reads it completes first); does not block the host. */
 int rcwa_geometry_destroy(rcwa_geometry* geom);
 /* Sweep on a prepared geometry.  sources: host array.  R_dev/T_dev: device
  * arrays [n_sources][Q*P]; tot_dev: device [n_sources][2] (R_tot, T_tot);

@@ -87,6 +87,21 @@ int rcwa_context_create(int device, rcwa_context** out) {
     return RCWA_ERR_CUDA;
   }
   c->stream = c->own_stream;
+  {
+    // geometries and result buffers come from the device's default
+    // stream-ordered pool; keep up to 1 GiB of it cached between calls so
+    // that repeated solves do not return memory to the driver each time
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = 0;
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      if (keep < (1ull << 30)) {
+        keep = 1ull << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+    }
+    cudaGetLastError();
+  }
   c->launches_at_create = launch_count();
   *out = c;
   return RCWA_OK;
@@ -142,8 +157,7 @@ int rcwa_geometry_create(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_
 
 int rcwa_geometry_destroy(rcwa_geometry* g) {
   if (!g) return RCWA_OK;
-  if (g->ctx) cudaStreamSynchronize(g->ctx->stream);
-  geometry_free(g);
+  geometry_free(g);   // stream-ordered frees on the context stream
   delete g;
   return RCWA_OK;
 }
@@ -168,8 +182,8 @@ int rcwa_solve_sweep(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_sour
   double *dR = nullptr, *dT = nullptr, *dtot = nullptr;
   uint32_t* dst = nullptr;
   const size_t nR = (size_t)n_sources * N;
-  cudaError_t e = cudaMalloc(&dR, 2 * nR * sizeof(double) + 2 * n_sources * sizeof(double) +
-                                      n_sources * sizeof(uint32_t) + 512);
+  cudaError_t e = cudaMallocAsync((void**)&dR, 2 * nR * sizeof(double) + 2 * n_sources * sizeof(double) +
+                                                    n_sources * sizeof(uint32_t) + 512, ctx->stream);
   if (e != cudaSuccess) {
     rcwa_geometry_destroy(g);
     set_last_error("result allocation failed: %s", cudaGetErrorString(e));
@@ -195,7 +209,7 @@ int rcwa_solve_sweep(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_sour
       rc = RCWA_ERR_CUDA;
     }
   }
-  cudaFree(dR);
+  cudaFreeAsync(dR, ctx->stream);
   rcwa_geometry_destroy(g);
   if (rc) return rc;
   bool any = false;

@@ -45,8 +45,10 @@ int zgemm_tc(cudaStream_t s, const ZGemm& g, int* err);
 int* tc_error_flag();   // device flag of the current device (set-up once per device)
 
 // X = A^-1 B on the augmented [A | B] (n x (n+nrhs), column-major, ld >= n).
+// tc = 1 runs the trailing and back-substitution updates as split-TF32
+// tensor-core GEMMs (mixed-precision mode).
 int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch,
-          int* piv, uint32_t* status);
+          int* piv, uint32_t* status, int tc = 0);
 
 // Blocked Hessenberg reduction of packed A (zero below the subdiagonal on
 // return) and Z = Q; V is an n x n scratch per matrix, ws hess_ws_bytes().

@@ -67,10 +67,11 @@ static double2 c2(const rcwa_complex& c) { return make_double2(c.re, c.im); }
 
 void geometry_free(rcwa_geometry* g) {
   if (!g) return;
-  if (g->erc) cudaFree(g->erc);
-  if (g->urc) cudaFree(g->urc);
-  if (g->einv) cudaFree(g->einv);
-  if (g->uinv) cudaFree(g->uinv);
+  const cudaStream_t s = g->ctx ? g->ctx->stream : nullptr;
+  if (g->erc) cudaFreeAsync(g->erc, s);
+  if (g->urc) cudaFreeAsync(g->urc, s);
+  if (g->einv) cudaFreeAsync(g->einv, s);
+  if (g->uinv) cudaFreeAsync(g->uinv, s);
   g->erc = g->urc = g->einv = g->uinv = nullptr;
 }
 
@@ -161,10 +162,10 @@ int geometry_build(rcwa_context* ctx, rcwa_geometry* g, const rcwa_stack* st,
   }
 
   geometry_free(g);
-  RCWA_CUDA_TRY(cudaMalloc(&g->erc, nl * NN * sizeof(double2)));
-  RCWA_CUDA_TRY(cudaMalloc(&g->urc, nl * NN * sizeof(double2)));
-  RCWA_CUDA_TRY(cudaMalloc(&g->einv, nl * NN * sizeof(double2)));
-  RCWA_CUDA_TRY(cudaMalloc(&g->uinv, nl * NN * sizeof(double2)));
+  RCWA_CUDA_TRY(cudaMallocAsync((void**)&g->erc, nl * NN * sizeof(double2), s));
+  RCWA_CUDA_TRY(cudaMallocAsync((void**)&g->urc, nl * NN * sizeof(double2), s));
+  RCWA_CUDA_TRY(cudaMallocAsync((void**)&g->einv, nl * NN * sizeof(double2), s));
+  RCWA_CUDA_TRY(cudaMallocAsync((void**)&g->uinv, nl * NN * sizeof(double2), s));
   // ConvMat for er and ur of every layer (main.cpp:126-138)
   rc = convmat(s, der, nl, st->nx, st->ny, d, g->erc, scr);
   if (rc) return rc;
@@ -227,6 +228,7 @@ int star_product(rcwa_context* ctx, int B, int n, SMat& A, const SMat& Bm, doubl
     g.B = Y; g.ldb = n; g.sB = sY;
     g.C = C; g.ldc = n; g.sC = sC;
     g.batch = B;
+    g.tc = ctx->tc;
     return zgemm(s, g);
   };
   const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
@@ -238,7 +240,7 @@ int star_product(rcwa_context* ctx, int B, int n, SMat& A, const SMat& Bm, doubl
   if ((rc = copy_blocks(s, augG + nn, s3, A.p[2], A.s[2], nn, B))) return rc;
   if ((rc = copy_blocks(s, augG + 2 * nn, s3, A.p[3], A.s[3], nn, B))) return rc;
   // F^-1 [B11 B12], G^-1 [A21 A22] (:605-611), both systems in one batch
-  if ((rc = zgesv(s, n, 2 * n, augFG, n, s3, 2 * B, piv, status))) return rc;
+  if ((rc = zgesv(s, n, 2 * n, augFG, n, s3, 2 * B, piv, status, ctx->tc))) return rc;
   // note: status is indexed per system; the caller ORs the two halves.
   const double2* X1 = augF + nn;      // F^-1 B11
   const double2* X2 = augF + 2 * nn;  // F^-1 B12
@@ -401,11 +403,12 @@ int patterned_layer(rcwa_context* ctx, const rcwa_geometry* g, int l, Plan& pl,
   gm.B = pl.augWV; gm.ldb = n; gm.sB = s2;
   gm.C = augV; gm.ldc = n; gm.sC = s2;
   gm.dr = pl.ilam; gm.sdr = n;
+  gm.tc = ctx->tc;
   if ((rc = zgemm(s, gm))) return rc;
   // W^-1, V^-1 (:335-336), one batched solve for both
   if ((rc = set_identity(s, pl.augWV, n, n, s2, 2 * n, n, 2 * B, one))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, n, pl.augWV, n, s2, 2 * B, pl.piv, pl.st))) return rc;
+  if ((rc = zgesv(s, n, n, pl.augWV, n, s2, 2 * B, pl.piv, pl.st, ctx->tc))) return rc;
   if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
   // A = W^-1 W0 + V^-1 V0 -> s1, B -> s0 (:337-338)
   if ((rc = assemble_ab(s, B, d, pl.augWV + nn, s2, augV + nn, s2, pl.wv.V0, pl.s1, pl.s0))) return rc;
@@ -413,7 +416,7 @@ int patterned_layer(rcwa_context* ctx, const rcwa_geometry* g, int l, Plan& pl,
   if ((rc = copy_blocks(s, pl.augA, s2, pl.s1, nn, nn, B))) return rc;
   if ((rc = set_identity(s, pl.augA, n, n, s2, 2 * n, n, B, one))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, n, pl.augA, n, s2, B, pl.piv, pl.st))) return rc;
+  if ((rc = zgesv(s, n, n, pl.augA, n, s2, B, pl.piv, pl.st, ctx->tc))) return rc;
   if ((rc = fold_status(s, status, pl.st, B, 1))) return rc;
   const double2* Ai = pl.augA + nn;
   // T1 = B A^-1 X -> s2   (X diag: column scaling)
@@ -423,6 +426,7 @@ int patterned_layer(rcwa_context* ctx, const rcwa_geometry* g, int l, Plan& pl,
   gm.B = Ai; gm.ldb = n; gm.sB = s2;
   gm.C = pl.s2; gm.ldc = n; gm.sC = nn;
   gm.dr = pl.X; gm.sdr = n;
+  gm.tc = ctx->tc;
   if ((rc = zgemm(s, gm))) return rc;
   // D = A - X T1 B -> augD[0] (:346)
   if ((rc = copy_blocks(s, pl.augD, s3, pl.s1, nn, nn, B))) return rc;
@@ -433,12 +437,14 @@ int patterned_layer(rcwa_context* ctx, const rcwa_geometry* g, int l, Plan& pl,
   gm.B = pl.s0; gm.ldb = n; gm.sB = nn;
   gm.C = pl.augD; gm.ldc = n; gm.sC = s3;
   gm.dl = pl.X; gm.sdl = n;
+  gm.tc = ctx->tc;
   if ((rc = zgemm(s, gm))) return rc;
   // R1 = X T1 A - B -> augD[1] (:347)
   if ((rc = copy_blocks(s, pl.augD + nn, s3, pl.s0, nn, nn, B))) return rc;
   gm.alpha = one; gm.beta = mone;
   gm.B = pl.s1;
   gm.C = pl.augD + nn;
+  gm.tc = ctx->tc;
   if ((rc = zgemm(s, gm))) return rc;
   // T3 = A^-1 B -> s3 ; R2 = A - B T3 -> s1 (in place) (:348)
   gm = ZGemm();
@@ -446,17 +452,19 @@ int patterned_layer(rcwa_context* ctx, const rcwa_geometry* g, int l, Plan& pl,
   gm.A = Ai; gm.lda = n; gm.sA = s2;
   gm.B = pl.s0; gm.ldb = n; gm.sB = nn;
   gm.C = pl.s3; gm.ldc = n; gm.sC = nn;
+  gm.tc = ctx->tc;
   if ((rc = zgemm(s, gm))) return rc;
   gm.alpha = mone; gm.beta = one;
   gm.A = pl.s0; gm.sA = nn;
   gm.B = pl.s3; gm.sB = nn;
   gm.C = pl.s1;
+  gm.tc = ctx->tc;
   if ((rc = zgemm(s, gm))) return rc;
   // X R2 -> augD[2]; then [D | R1 | X R2] -> S11 = D^-1 R1 (:347), S12 = D^-1 X R2 (:348)
   if ((rc = scale_rows(s, pl.s1, n, n, n, nn, pl.X, n, B))) return rc;
   if ((rc = copy_blocks(s, pl.augD + 2 * nn, s3, pl.s1, nn, nn, B))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, 2 * n, pl.augD, n, s3, B, pl.piv, pl.st))) return rc;
+  if ((rc = zgesv(s, n, 2 * n, pl.augD, n, s3, B, pl.piv, pl.st, ctx->tc))) return rc;
   (void)zero;
   return fold_status(s, status, pl.st, B, 1);
 }
@@ -484,9 +492,10 @@ int star_product_bd(rcwa_context* ctx, int B, const ModeDims& d, SMat& A, const 
   if ((rc = bd_apply(s, 1, N, n, n, L11, sL, A.p[3], n, A.s[3], augG, n, s3, mone, zero, 1, B))) return rc;
   if ((rc = copy_blocks(s, augG + nn, s3, A.p[2], A.s[2], nn, B))) return rc;
   if ((rc = copy_blocks(s, augG + 2 * nn, s3, A.p[3], A.s[3], nn, B))) return rc;
-  if ((rc = zgesv(s, n, 2 * n, augFG, n, s3, 2 * B, piv, st))) return rc;
+  if ((rc = zgesv(s, n, 2 * n, augFG, n, s3, 2 * B, piv, st, ctx->tc))) return rc;
   ZGemm g;
   g.m = n; g.n = n; g.k = n; g.batch = B;
+  g.tc = ctx->tc;
   // S11 = A11 + A12 X1
   g.alpha = one; g.beta = one;
   g.A = A.p[1]; g.lda = n; g.sA = A.s[1];
@@ -537,6 +546,7 @@ int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, c
     g.A = X; g.lda = n; g.sA = sX;
     g.B = Y; g.ldb = n; g.sB = sY;
     g.C = C; g.ldc = n; g.sC = sC;
+    g.tc = ctx->tc;
     return zgemm(s, g);
   };
   // [G1 | R22 D12 | R21 E] in augFG (stride 6n^2)
@@ -548,7 +558,7 @@ int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, c
   if ((rc = bd_apply(s, 1, N, n, n, R22, sP, D.p[0], n, D.s[0], augA, n, s2, mone, zero, 1, B))) return rc;
   if ((rc = gemm(n, 2, augA + nn, s2, D.p[0], D.s[0], u, s6, zero))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, n + 2, augFG, n, s6, B, piv, st))) return rc;
+  if ((rc = zgesv(s, n, n + 2, augFG, n, s6, B, piv, st, ctx->tc))) return rc;
   if ((rc = fold_status(s, status, st, B, 1))) return rc;
   // S'22 -> s0, S'21 E -> s1
   if ((rc = copy_blocks(s, s0, nn, D.p[3], D.s[3], nn, B))) return rc;
@@ -561,14 +571,14 @@ int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, c
   if ((rc = bd_apply(s, 1, N, n, n, T11, sP, s0, n, nn, augG2, n, s2, mone, zero, 1, B))) return rc;
   if ((rc = copy_blocks(s, augG2 + nn, s2, s1, nn, c2, B))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, 2, augWV, n, s2, 2 * B, piv, st))) return rc;
+  if ((rc = zgesv(s, n, 2, augWV, n, s2, 2 * B, piv, st, ctx->tc))) return rc;
   if ((rc = fold_status(s, status, st, B, 2))) return rc;
   // S''21 E = T21 z
   if ((rc = bd_apply(s, 0, N, n, 2, T21, sP, augG2 + nn, n, s2, S21E, n, c2, one, zero, 0, B))) return rc;
   // v = D11 R21 E + D12 x, then q = F1^-1 v
   if ((rc = gemm(n, 2, augA + nn, s2, D.p[1], D.s[1], augWV + nn, s2, one))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, 2, augA, n, s2, B, piv, st))) return rc;
+  if ((rc = zgesv(s, n, 2, augA, n, s2, B, piv, st, ctx->tc))) return rc;
   if ((rc = fold_status(s, status, st, B, 1))) return rc;
   // S''11 E = R11 E + R12 q
   if ((rc = bd_cols(s, N, a, R11, sP, S11E, n, c2, one, zero, B))) return rc;
@@ -671,11 +681,25 @@ static int sweep_chunk(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_sou
 
 int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* sources, int B,
                  int precision, double* R, double* T, double* tot, uint32_t* status) {
-  if (precision != RCWA_PREC_FP64) {
-    set_last_error("precision mode %d is not available in this build", precision);
+  if (precision != RCWA_PREC_FP64 && precision != RCWA_PREC_MIXED) {
+    set_last_error("unknown precision mode %d", precision);
     return RCWA_ERR_INVALID;
   }
   if (B <= 0) return RCWA_OK;
+  int* tc_err = nullptr;
+  if (precision == RCWA_PREC_MIXED) {
+    tc_err = tc_error_flag();
+    if (!tc_err) {
+      set_last_error("tensor-core GEMM error flag unavailable on this device");
+      return RCWA_ERR_CUDA;
+    }
+    RCWA_CUDA_TRY(cudaMemsetAsync(tc_err, 0, sizeof(int), ctx->stream));
+  }
+  struct TcScope {  // the flag never outlives this sweep, also on early return
+    rcwa_context* c;
+    ~TcScope() { c->tc = 0; }
+  } tc_scope{ctx};
+  ctx->tc = precision == RCWA_PREC_MIXED ? 1 : 0;
   const ModeDims& d = g->d;
   // chunk size from the memory budget
   size_t budget = ctx->mem_budget;
@@ -693,6 +717,15 @@ int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* s
     int rc = sweep_chunk(ctx, g, sources + b0, bc, R + b0 * N, T + b0 * N, tot + 2LL * b0,
                          status + b0);
     if (rc) return rc;
+  }
+  if (tc_err) {
+    int h = 0;
+    RCWA_CUDA_TRY(cudaMemcpyAsync(&h, tc_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    RCWA_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (h) {
+      set_last_error("tensor-core GEMM: a bounded mbarrier wait expired");
+      return RCWA_ERR_CUDA;
+    }
   }
   return RCWA_OK;
 }

@@ -20,6 +20,10 @@ struct rcwa_context {
   size_t pinned_bytes = 0;
   uint64_t launches_at_create = 0;
   size_t mem_budget = 0;  // bytes usable for one sweep chunk (0 = auto)
+  // 1 while a mixed-precision sweep runs: the S-matrix algebra (layer
+  // assembly, star products, their LU solves) uses split-TF32 tensor-core
+  // GEMMs; Omega^2 and the eigensolver stay FP64
+  int tc = 0;
 };
 
 struct rcwa_geometry {

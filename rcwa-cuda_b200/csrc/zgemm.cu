@@ -1,4 +1,4 @@
-// Batched complex128 GEMM on FP64 CUDA cores.
+// Batched complex128 GEMM.
 //
 //   C[b] = alpha * diag(dl[b]) * A[b] * B[b] * diag(dr[b]) + beta * C[b]
 //
@@ -8,11 +8,13 @@
 // the reference's asDiagonal() products (rcwa.cpp:273-285, 329, 339) into the
 // epilogue so no dense diagonal matrix is ever materialised.
 //
-// Tiling: 64x64 C tile per CTA, K step 8, 256 threads as 16x16, each thread a
-// 4x4 complex micro-tile (rows tx+16i, cols ty+16j so that warp stores are
-// coalesced along the column).  A and B tiles are staged into shared memory
-// with cp.async (16-byte copies, zero-filled outside the matrix) and double
-// buffered.
+// Two FP64 kernels: the default runs on the FP64 tensor cores (DMMA, below);
+// a CUDA-core kernel (64x64 C tile, K step 8, 256 threads as 16x16, each a
+// 4x4 complex micro-tile) is kept as the alternative.  Both stage A and B
+// tiles with cp.async (16-byte copies, zero-filled outside the matrix).
+// tcgen05 has no FP64 kind, so FP64 tensor work on sm_100a is mma.sync DMMA.
+#include <cstring>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -35,42 +37,46 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // OPA / OPB: 0 = the operand as stored, 1 = its conjugate transpose.
-template <int OPA, int OPB>
-__global__ void __launch_bounds__(NT, 2)
+// MI = complex rows per thread: the CTA tile is (16 MI) x 64.
+template <int OPA, int OPB, int MI>
+__global__ void __launch_bounds__(NT, (MI > 4 ? 1 : 2))
 zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, int lda,
              long long sA, const double2* __restrict__ B, int ldb, long long sB, double2 beta,
              double2* __restrict__ C, int ldc, long long sC, const double2* __restrict__ dl,
              long long sdl, const double2* __restrict__ dr, long long sdr) {
-  __shared__ __align__(16) double2 As[2][BK][BM];
+  constexpr int TM = 16 * MI;
+  __shared__ __align__(16) double2 As[2][BK][TM];
   __shared__ __align__(16) double2 Bs[2][BK][BN];
 
   const int b = blockIdx.z;
   A += (long long)b * sA;
   B += (long long)b * sB;
   C += (long long)b * sC;
-  const int m0 = blockIdx.y * BM;
+  const int m0 = blockIdx.y * TM;
   const int n0 = blockIdx.x * BN;
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
 
-  double2 acc[4][4];
+  double2 acc[MI][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < MI; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = cmk(0.0, 0.0);
 
   auto load_tile = [&](int buf, int k0) {
+    // A tile: TM rows x 8 k (consecutive threads walk the contiguous index)
+#pragma unroll
+    for (int h = 0; h < TM * BK / NT; ++h) {
+      const int e = tid + h * NT;
+      const int r = OPA ? (e >> 3) : (e % TM), kk = OPA ? (e & 7) : (e / TM);
+      const int gr = m0 + r, gk = k0 + kk;
+      const bool pa = (gr < m) && (gk < k);
+      const double2* srcA = pa ? (OPA ? A + (long long)gr * lda + gk : A + (long long)gk * lda + gr) : A;
+      cp_async16(&As[buf][kk][r], srcA, pa);
+    }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       int e = tid + h * NT;
-      // A tile: 64 rows x 8 k (consecutive threads walk the contiguous index)
-      {
-        const int r = OPA ? (e >> 3) : (e & 63), kk = OPA ? (e & 7) : (e >> 6);
-        const int gr = m0 + r, gk = k0 + kk;
-        const bool pa = (gr < m) && (gk < k);
-        const double2* srcA = pa ? (OPA ? A + (long long)gr * lda + gk : A + (long long)gk * lda + gr) : A;
-        cp_async16(&As[buf][kk][r], srcA, pa);
-      }
       // B tile: 8 k x 64 cols
       {
         const int kb = OPB ? (e >> 6) : (e & 7), c = OPB ? (e & 63) : (e >> 3);
@@ -96,9 +102,9 @@ zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, 
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
-      double2 a[4], bb[4];
+      double2 a[MI], bb[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
+      for (int i = 0; i < MI; ++i) {
         a[i] = As[buf][kk][tx + 16 * i];
         if (OPA) a[i].y = -a[i].y;
       }
@@ -108,7 +114,7 @@ zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, 
         if (OPB) bb[j].y = -bb[j].y;
       }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < MI; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) cfma(acc[i][j], a[i], bb[j]);
     }
@@ -122,7 +128,7 @@ zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, 
     if (col >= n) continue;
     double2 sr = dr ? dr[(long long)b * sdr + col] : cmk(1.0, 0.0);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < MI; ++i) {
       int row = m0 + tx + 16 * i;
       if (row >= m) continue;
       double2 v = cmul(alpha, acc[i][j]);
@@ -136,37 +142,50 @@ zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, 
 }
 
 // ---------------------------------------------------------------------------
-// FP64 tensor-core variant: mma.sync m8n8k4 f64 (DMMA).  Same 64x64 CTA tile,
-// K step 8 and cp.async staging; 4 warps in a 2x2 grid, each computing a 32x32
+// FP64 tensor-core kernel: mma.sync m8n8k4 f64 (DMMA).  64x64 CTA tile, K step
+// 8, a 4-stage cp.async pipeline; 4 warps in a 2x2 grid, each computing a 32x32
 // complex tile as 4x4 blocks of 8x8.  A complex 8x8x4 block product is four
 // real DMMAs:  Cr += Ar Br + (-Ai) Bi,  Ci += Ar Bi + Ai Br.
 // Fragment layout of m8n8k4.f64: A(row = lane/4, k = lane%4),
 // B(k = lane%4, col = lane/4), C(row = lane/4, cols 2*(lane%4) + {0,1}).
 // ---------------------------------------------------------------------------
-constexpr int DNT = 128;
-
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
   asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
       : "+d"(c[0]), "+d"(c[1])
       : "d"(a), "d"(b));
 }
 
-template <int OPA, int OPB>
-__global__ void __launch_bounds__(DNT, 2)
+// WM warps along M x 2 along N, each a 32x32 complex tile: CTA tile
+// (32 WM) x 64, 64 WM threads.
+template <int OPA, int OPB, int WM, int ST>
+__global__ void __launch_bounds__(64 * WM, (WM > 2 ? 1 : 2))
 zgemm_dmma_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, int lda,
                   long long sA, const double2* __restrict__ B, int ldb, long long sB, double2 beta,
                   double2* __restrict__ C, int ldc, long long sC, const double2* __restrict__ dl,
                   long long sdl, const double2* __restrict__ dr, long long sdr) {
-  __shared__ __align__(16) double2 As[2][BK][BM];
-  __shared__ __align__(16) double2 Bs[2][BK][BN];
+  constexpr int DT = 64 * WM, TM = 32 * WM;
+  // rows padded by two elements: the fragment loads (4 k x 8 rows per
+  // quarter-warp pattern) then hit distinct shared-memory banks
+  constexpr int TMP = TM + 2, BNP = BN + 2;
+  extern __shared__ __align__(16) double2 dsm[];
+  double2 (*As)[BK][TMP] = reinterpret_cast<double2 (*)[BK][TMP]>(dsm);
+  double2 (*Bs)[BK][BNP] = reinterpret_cast<double2 (*)[BK][BNP]>(dsm + ST * BK * TMP);
   const int b = blockIdx.z;
   A += (long long)b * sA;
   B += (long long)b * sB;
   C += (long long)b * sC;
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int m0 = blockIdx.y * TM, n0 = blockIdx.x * BN;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp & 1, wn = warp >> 1;
+  const int wm = warp % WM, wn = warp / WM;
   const int lr = lane >> 2, lk = lane & 3;
+  // 8x8 blocks of this warp that hold any row < m / column < n (warp-uniform):
+  // edge tiles skip the products of blocks entirely outside the matrix
+  int live_i = 0, live_j = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    live_i |= (m0 + wm * 32 + q * 8 < m) ? (1 << q) : 0;
+    live_j |= (n0 + wn * 32 + q * 8 < n) ? (1 << q) : 0;
+  }
 
   double cr[4][4][2], ci[4][4][2];
 #pragma unroll
@@ -179,37 +198,44 @@ zgemm_dmma_kernel(int m, int n, int k, double2 alpha, const double2* __restrict_
 
   auto load_tile = [&](int buf, int k0) {
 #pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const int e = tid + h * DNT;
-      {
-        const int r = OPA ? (e >> 3) : (e & 63), kk = OPA ? (e & 7) : (e >> 6);
-        const int gr = m0 + r, gk = k0 + kk;
-        const bool pa = (gr < m) && (gk < k);
-        const double2* srcA = pa ? (OPA ? A + (long long)gr * lda + gk : A + (long long)gk * lda + gr) : A;
-        cp_async16(&As[buf][kk][r], srcA, pa);
-      }
-      {
-        const int kb = OPB ? (e >> 6) : (e & 7), c = OPB ? (e & 63) : (e >> 3);
-        const int gk2 = k0 + kb, gc = n0 + c;
-        const bool pb = (gk2 < k) && (gc < n);
-        const double2* srcB = pb ? (OPB ? B + (long long)gk2 * ldb + gc : B + (long long)gc * ldb + gk2) : B;
-        cp_async16(&Bs[buf][kb][c], srcB, pb);
-      }
+    for (int h = 0; h < TM * BK / DT; ++h) {
+      const int e = tid + h * DT;
+      const int r = OPA ? (e >> 3) : (e % TM), kk = OPA ? (e & 7) : (e / TM);
+      const int gr = m0 + r, gk = k0 + kk;
+      const bool pa = (gr < m) && (gk < k);
+      const double2* srcA = pa ? (OPA ? A + (long long)gr * lda + gk : A + (long long)gk * lda + gr) : A;
+      cp_async16(&As[buf][kk][r], srcA, pa);
+    }
+#pragma unroll
+    for (int h = 0; h < BN * BK / DT; ++h) {
+      const int e = tid + h * DT;
+      const int kb = OPB ? (e >> 6) : (e & 7), c = OPB ? (e & 63) : (e >> 3);
+      const int gk2 = k0 + kb, gc = n0 + c;
+      const bool pb = (gk2 < k) && (gc < n);
+      const double2* srcB = pb ? (OPB ? B + (long long)gk2 * ldb + gc : B + (long long)gc * ldb + gk2) : B;
+      cp_async16(&Bs[buf][kb][c], srcB, pb);
     }
     cp_async_commit();
   };
 
+  // ST-stage cp.async pipeline: tiles t+1 .. t+ST-1 are in flight while
+  // tile t is consumed (an empty group is committed past the end so the
+  // wait count stays fixed)
   const int ktiles = (k + BK - 1) / BK;
-  if (ktiles > 0) load_tile(0, 0);
+#pragma unroll
+  for (int p = 0; p < ST - 1; ++p) {
+    if (p < ktiles) load_tile(p, p * BK);
+    else cp_async_commit();
+  }
   for (int t = 0; t < ktiles; ++t) {
-    const int buf = t & 1;
-    if (t + 1 < ktiles) {
-      load_tile(buf ^ 1, (t + 1) * BK);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
+    const int buf = t % ST;
+    cp_async_wait<ST - 2>();
     __syncthreads();
+    {
+      const int tn = t + ST - 1;   // refills the buffer consumed at t-1
+      if (tn < ktiles) load_tile(tn % ST, tn * BK);
+      else cp_async_commit();
+    }
 #pragma unroll
     for (int kq = 0; kq < BK / 4; ++kq) {
       double ar[4], ai[4], nai[4], br[4], bi[4];
@@ -230,13 +256,13 @@ zgemm_dmma_kernel(int m, int n, int k, double2 alpha, const double2* __restrict_
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
+          if (!((live_i >> i) & (live_j >> j) & 1)) continue;   // block beyond m or n
           dmma(cr[i][j], ar[i], br[j]);
           dmma(cr[i][j], nai[i], bi[j]);
           dmma(ci[i][j], ar[i], bi[j]);
           dmma(ci[i][j], ai[i], br[j]);
         }
     }
-    __syncthreads();
   }
 
   const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
@@ -261,16 +287,45 @@ zgemm_dmma_kernel(int m, int n, int k, double2 alpha, const double2* __restrict_
     }
 }
 
-// Implementation switch (read once): RCWA_ZGEMM=dmma selects the DMMA kernel,
-// the default is the CUDA-core kernel (on the solve's GEMM mix it measured
-// 13.8 TFLOP/s against 12.3 for the DMMA kernel on B200).
-int gemm_impl() {
+// Kernel choice.  Default: the DMMA kernel for k > 64 and the CUDA-core
+// kernel for the rank-k updates (k <= 64) of the LU factorisations -- in the
+// C2 sweep on B200 the DMMA kernel ran the k = 450 GEMMs at 21.8 TFLOP/s
+// (CUDA cores: 16.1) and the rank-32 updates at 9.0 (CUDA cores: 12.0).
+// RCWA_ZGEMM=ffma or =dmma (read once) forces one kernel for every shape.
+int gemm_impl(int k) {
   static int impl = -1;
   if (impl < 0) {
     const char* e = getenv("RCWA_ZGEMM");
-    impl = (e && e[0] == 'd') ? 1 : 0;
+    impl = (e && strcmp(e, "ffma") == 0) ? 1 : (e && strcmp(e, "dmma") == 0) ? 2 : 0;
   }
-  return impl;
+  if (impl == 0) return k > 64 ? 0 : 1;
+  return impl == 2 ? 0 : 1;
+}
+
+template <int WM, int ST>
+int launch_dmma(cudaStream_t s, const ZGemm& g, dim3 grid) {
+  constexpr int smem = ST * BK * (32 * WM + 2 + BN + 2) * (int)sizeof(double2);
+  static bool attr[64] = {};   // per device
+  int dev = 0;
+  RCWA_CUDA_TRY(cudaGetDevice(&dev));
+  if (smem > 48 * 1024 && (dev >= 64 || !attr[dev])) {
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(zgemm_dmma_kernel<0, 0, WM, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(zgemm_dmma_kernel<1, 0, WM, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(zgemm_dmma_kernel<0, 1, WM, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(zgemm_dmma_kernel<1, 1, WM, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    if (dev < 64) attr[dev] = true;
+  }
+  grid.y = cdiv_up(g.m, 32 * WM);
+  const int kk = g.k < 0 ? 0 : g.k;
+#define RCWA_DMMA_ARGS                                                                          \
+  g.m, g.n, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
+      g.dr, g.sdr
+  if (g.opA == 0 && g.opB == 0) zgemm_dmma_kernel<0, 0, WM, ST><<<grid, 64 * WM, smem, s>>>(RCWA_DMMA_ARGS);
+  else if (g.opA == 1 && g.opB == 0) zgemm_dmma_kernel<1, 0, WM, ST><<<grid, 64 * WM, smem, s>>>(RCWA_DMMA_ARGS);
+  else if (g.opA == 0 && g.opB == 1) zgemm_dmma_kernel<0, 1, WM, ST><<<grid, 64 * WM, smem, s>>>(RCWA_DMMA_ARGS);
+  else zgemm_dmma_kernel<1, 1, WM, ST><<<grid, 64 * WM, smem, s>>>(RCWA_DMMA_ARGS);
+#undef RCWA_DMMA_ARGS
+  return RCWA_OK;
 }
 
 }  // namespace
@@ -289,25 +344,25 @@ int zgemm(cudaStream_t s, const ZGemm& g) {
   dim3 grid(cdiv_up(g.n, BN), cdiv_up(g.m, BM), g.batch);
   void* tok = prof_begin(s);
   const int kk = g.k < 0 ? 0 : g.k;
+  int rc = RCWA_OK;
 #define RCWA_ZGEMM_ARGS                                                                          \
   g.m, g.n, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
       g.dr, g.sdr
-  if (gemm_impl() == 1) {
-    if (g.opA == 0 && g.opB == 0) zgemm_dmma_kernel<0, 0><<<grid, DNT, 0, s>>>(RCWA_ZGEMM_ARGS);
-    else if (g.opA == 1 && g.opB == 0) zgemm_dmma_kernel<1, 0><<<grid, DNT, 0, s>>>(RCWA_ZGEMM_ARGS);
-    else if (g.opA == 0 && g.opB == 1) zgemm_dmma_kernel<0, 1><<<grid, DNT, 0, s>>>(RCWA_ZGEMM_ARGS);
-    else zgemm_dmma_kernel<1, 1><<<grid, DNT, 0, s>>>(RCWA_ZGEMM_ARGS);
+  if (gemm_impl(kk) == 0) {
+    if ((rc = launch_dmma<2, 4>(s, g, grid))) return rc;
   } else {
-    if (g.opA == 0 && g.opB == 0) zgemm_kernel<0, 0><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
-    else if (g.opA == 1 && g.opB == 0) zgemm_kernel<1, 0><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
-    else if (g.opA == 0 && g.opB == 1) zgemm_kernel<0, 1><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
-    else zgemm_kernel<1, 1><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
+    if (g.opA == 0 && g.opB == 0) zgemm_kernel<0, 0, 4><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
+    else if (g.opA == 1 && g.opB == 0) zgemm_kernel<1, 0, 4><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
+    else if (g.opA == 0 && g.opB == 1) zgemm_kernel<0, 1, 4><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
+    else zgemm_kernel<1, 1, 4><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
   }
 #undef RCWA_ZGEMM_ARGS
-  prof_end(s, tok, "zgemm");
+  // rank-k updates (k <= 64: the LU panel updates) are a family of their own
+  const char* fam = kk <= 64 ? "zgemm_rank" : "zgemm";
+  prof_end(s, tok, fam);
   if (tok) {
     // algorithmic flops of this launch, for the roofline (8 m n k per matrix)
-    prof_add_flops("zgemm", 8.0 * g.m * (double)g.n * (double)(g.k < 0 ? 0 : g.k) * g.batch);
+    prof_add_flops(fam, 8.0 * g.m * (double)g.n * (double)kk * g.batch);
   }
   count_launch();
   RCWA_LAUNCH_CHECK();

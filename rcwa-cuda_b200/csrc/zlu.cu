@@ -202,7 +202,7 @@ lu_usolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int j, int 
 }  // namespace
 
 int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch,
-          int* piv, uint32_t* status) {
+          int* piv, uint32_t* status, int tc) {
   if (n <= 0 || batch <= 0) return RCWA_OK;
   const int ncols = n + nrhs;
   for (int j = 0; j < n; j += NB) {
@@ -235,6 +235,7 @@ int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride,
         gm.ldc = ld;
         gm.sC = stride;
         gm.batch = batch;
+        gm.tc = tc;
         int rc = zgemm(s, gm);
         if (rc) return rc;
       }
@@ -266,6 +267,7 @@ int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride,
       gm.ldc = ld;
       gm.sC = stride;
       gm.batch = batch;
+      gm.tc = tc;
       int rc = zgemm(s, gm);
       if (rc) return rc;
     }

@@ -630,13 +630,13 @@ int schur_launch(cudaStream_t s, double2* H, int ld, long long sH, int n, double
                  long long slam, uint32_t* status, int batch) {
   void* tok = prof_begin(s);
   constexpr size_t stage_bytes = sizeof(double2) * (NT / 32) * 32 * NR;
-  static bool attr_set[64] = {};
+  static bool attr_set[64] = {};   // the attribute is per device
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && !attr_set[dev]) {
+  RCWA_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 64 || !attr_set[dev]) {
     RCWA_CUDA_TRY(cudaFuncSetAttribute(schur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)stage_bytes));
-    attr_set[dev] = true;
+    if (dev < 64) attr_set[dev] = true;
   }
   schur_kernel<<<batch, NT, stage_bytes, s>>>(H, ld, sH, n, Z, lam, slam, status, 100);
   prof_end(s, tok, "schur");

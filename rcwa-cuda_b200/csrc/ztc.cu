@@ -245,10 +245,12 @@ int zgemm_tc(cudaStream_t s, const ZGemm& g, int* err) {
     set_last_error("zgemm_tc: transposed operands are not supported");
     return RCWA_ERR_INVALID;
   }
-  static bool attr = false;
-  if (!attr) {
+  static bool attr[64] = {};   // the attribute is per device
+  int dev = 0;
+  RCWA_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 64 || !attr[dev]) {
     RCWA_CUDA_TRY(cudaFuncSetAttribute(zgemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-    attr = true;
+    if (dev < 64) attr[dev] = true;
   }
   dim3 grid(cdiv_up(g.n, TBN), cdiv_up(g.m, TBM), g.batch);
   void* tok = prof_begin(s);
