@@ -273,3 +273,19 @@ def test_zero_thickness_and_single_uniform(ctx):
     a = ctx.solve_sweep(pa)
     b = ctx.solve_sweep(pb)
     assert np.abs(a[0] - b[0]).max() < 1e-11 and np.abs(a[1] - b[1]).max() < 1e-11
+
+
+@pytest.mark.parametrize("name", ["golden_small_c1", "golden_small_mixed"])
+def test_golden_fixtures(ctx, name):
+    """The CUDA path reproduces the committed fixtures (generated by the
+    oracle, tests/golden/make_golden.py) to 1e-10 per order."""
+    import os
+    from golden.make_golden import build_case
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    pb = build_case(name)
+    R, T, Rt, Tt, st = ctx.solve_sweep(pb)
+    assert not st.any()
+    assert np.abs(R - z["R"]).max() <= TOL_RT
+    assert np.abs(T - z["T"]).max() <= TOL_RT
+    assert np.abs(Rt - z["R_tot"]).max() <= TOL_RT
+    assert np.abs(Tt - z["T_tot"]).max() <= TOL_RT
