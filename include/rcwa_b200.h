@@ -137,6 +137,36 @@ int rcwa_solve_sweep_device(rcwa_context* ctx, const rcwa_geometry* geom,
                             double* R_dev, double* T_dev, double* tot_dev,
                             uint32_t* status_dev);
 
+/* ---- batches and serving ------------------------------------------------
+ * The reference solves one problem per call (main.cpp:111-191); these run
+ * many unrelated problems together.  Problems of equal shape (harmonic
+ * orders, layer count, grid size, port media, which layers are uniform) are
+ * solved as one batched GPU solve. */
+/* n problems: stacks[i], sources[i], params[i]; out[i] receives problem i.
+ * Returns RCWA_ERR_NUMERIC when any out[i].status is nonzero. */
+int rcwa_solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks,
+                     const rcwa_source* sources, const rcwa_params* params, int precision,
+                     rcwa_result* out);
+/* Serving loop: a worker thread with its own context on `device` takes all
+ * queued requests (up to max_batch) at the start of each batch and solves
+ * them with rcwa_solve_batch (continuous batching).  At most max_queue
+ * requests wait at a time. */
+int rcwa_server_create(int device, int max_batch, int max_queue, int precision,
+                       rcwa_server** out);
+/* Queues one request; the stack's arrays are copied (the caller may free them
+ * on return).  RCWA_ERR_BUSY when max_queue requests are waiting. */
+int rcwa_server_submit(rcwa_server* srv, const rcwa_stack* stack, const rcwa_source* source,
+                       const rcwa_params* params, uint64_t* ticket);
+/* *done = 1 once the request finished (wait != 0 blocks until then); out
+ * (optional; R/T caller arrays of Q*P doubles, each may be NULL) receives the
+ * result and the ticket is released.  Returns the request's own code once
+ * done; RCWA_ERR_NOTFOUND for an unknown or already collected ticket. */
+int rcwa_server_poll(rcwa_server* srv, uint64_t ticket, int wait, rcwa_result* out, int* done);
+/* Completed requests and their submit-to-completion latency p50 / p99 (ms). */
+int rcwa_server_stats(rcwa_server* srv, uint64_t* completed, double* p50_ms, double* p99_ms);
+/* Finishes the queued requests, stops the worker, releases the context. */
+int rcwa_server_destroy(rcwa_server* srv);
+
 /* ---- step-level entry points (host pointers; one per reference function) */
 /* ConvMat, rcwa.cpp:6-82: out is PQ x PQ column-major. */
 int rcwa_convmat(rcwa_context* ctx, const rcwa_complex* field, int layer, int nx, int ny,

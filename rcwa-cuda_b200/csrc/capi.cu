@@ -229,6 +229,20 @@ int rcwa_solve(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_source* so
   return rcwa_solve_sweep(ctx, stack, source, 1, params, precision, out);
 }
 
+int rcwa_solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_source* sources,
+                     const rcwa_params* params, int precision, rcwa_result* out) {
+  CHECK_ARG(ctx && stacks && sources && params && out, "NULL argument");
+  CHECK_ARG(n >= 0, "negative problem count");
+  for (int i = 0; i < n; ++i) {
+    int rc = check_stack(stacks + i);
+    if (!rc) rc = check_params(params + i);
+    if (rc) return rc;
+  }
+  if (n == 0) return RCWA_OK;
+  RCWA_CUDA_TRY(cudaSetDevice(ctx->device));
+  return solve_batch(ctx, n, stacks, sources, params, precision, 0, out);
+}
+
 // ---- step level -------------------------------------------------------------
 int rcwa_convmat(rcwa_context* ctx, const rcwa_complex* field, int layer, int nx, int ny,
                  int nx_harmonics, int ny_harmonics, rcwa_complex* out) {

@@ -73,8 +73,11 @@ int convmat(cudaStream_t s, const double2* grids, int nl, int nx, int ny, const 
 size_t convmat_scratch_bytes(int nl, int nx, int ny, const ModeDims& d);
 
 // Per-source wave vectors (rcwa.cpp:85-160) and gap modes (rcwa.cpp:163-234).
+// One solve's source plus its lattice periods: a sweep repeats the stack's
+// Lx/Ly in every entry; a batch of unrelated stacks carries each its own.
 struct SourceDev {
   double lambda0, theta, phi, pte, ptm;
+  double lx, ly;
 };
 struct WaveVecs {
   double2* Kx;      // [B][N]
@@ -84,17 +87,20 @@ struct WaveVecs {
   double2* V0;      // [B][4][N]: diagonals (11, 12, 21, 22) of the gap V0
   double2* kinc;    // [B][4]: k_inc x, y, z, (k0, 0)
 };
-int wave_vectors(cudaStream_t s, const SourceDev* src_dev, int B, double lx, double ly,
-                 const ModeDims& d, double2 er_ref, double2 ur_ref, double2 er_trn,
-                 double2 ur_trn, const WaveVecs& w, uint32_t* status);
+int wave_vectors(cudaStream_t s, const SourceDev* src_dev, int B, const ModeDims& d,
+                 double2 er_ref, double2 ur_ref, double2 er_trn, double2 ur_trn,
+                 const WaveVecs& w, uint32_t* status);
 
 // P and Q of a patterned layer (rcwa.cpp:262-286) from erc^-1 / urc^-1.
+// Item b reads its matrices at offset b * s_item (0: one set for all items).
 int assemble_pq(cudaStream_t s, int B, const ModeDims& d, const double2* erc, const double2* urc,
-                const double2* einv, const double2* uinv, const WaveVecs& w, double2* P,
-                double2* Qm);
+                const double2* einv, const double2* uinv, long long s_item, const WaveVecs& w,
+                double2* P, double2* Qm);
 // lam = usqrt(lam2), ilam = 1/lam, X = exp(-k0 t lam) (rcwa.cpp:317, 329, 339).
+// t_item (device, may be null): item b's thickness at t_item[b * t_stride].
 int layer_modes(cudaStream_t s, int B, int n, const double2* lam2, const double2* kinc,
-                double t, double2* lam, double2* ilam, double2* X);
+                double t, const double* t_item, int t_stride, double2* lam, double2* ilam,
+                double2* X);
 // A = Wi + Vi V0, B = Wi - Vi V0 (rcwa.cpp:335-338); Wi, Vi dense inverses.
 int assemble_ab(cudaStream_t s, int B, const ModeDims& d, const double2* Wi, long long sWi,
                 const double2* Vi, long long sVi, const double2* V0, double2* A, double2* Bm);
@@ -102,8 +108,11 @@ int assemble_ab(cudaStream_t s, int B, const ModeDims& d, const double2* Wi, lon
 // erc = eps I, urc = mu I; writes dense S11 and S12.
 // bd != 0 writes the 2x2-block-diagonal "BD" form: per block four diagonals
 // [X(i,i), X(i,i+N), X(i+N,i), X(i+N,i+N)] of length N (4N values).
+// eps_item / mu_item / t_item (device, may be null): per-item values at
+// [b * stride], replacing eps / mu / t.
 int uniform_layer(cudaStream_t s, int B, const ModeDims& d, double2 eps, double2 mu, double t,
-                  const WaveVecs& w, double2* S11, double2* S12, long long sS, int bd);
+                  const double2* eps_item, const double2* mu_item, const double* t_item,
+                  int stride, const WaveVecs& w, double2* S11, double2* S12, long long sS, int bd);
 // Reflection / transmission side S-matrices (rcwa.cpp:354-466), dense or BD.
 int port_smatrix(cudaStream_t s, int B, const ModeDims& d, int side, double2 er, double2 ur,
                  const WaveVecs& w, double2* S11, double2* S12, double2* S21, double2* S22,

@@ -132,7 +132,7 @@ __global__ void convmat_gather_kernel(const double2* __restrict__ Cg, int P, int
 // ---------------------------------------------------------------------------
 // K2: wave vectors (rcwa.cpp:85-160) and gap modes (rcwa.cpp:163-234).
 // ---------------------------------------------------------------------------
-__global__ void wavevec_kernel(const SourceDev* __restrict__ srcs, double lx, double ly, int nxh,
+__global__ void wavevec_kernel(const SourceDev* __restrict__ srcs, int nxh,
                                int nyh, int Q, int N, double2 er_ref, double2 ur_ref,
                                double2 er_trn, double2 ur_trn, WaveVecs w,
                                uint32_t* __restrict__ status) {
@@ -151,7 +151,7 @@ __global__ void wavevec_kernel(const SourceDev* __restrict__ srcs, double lx, do
     ki[2] = k0z;
     ki[3] = cmk(2.0 * kPi / sv.lambda0, 0.0);                        // k0, rcwa.hpp:92
   }
-  const double cx = -(sv.lambda0 / lx), cy = -(sv.lambda0 / ly);    // :110, :113
+  const double cx = -(sv.lambda0 / sv.lx), cy = -(sv.lambda0 / sv.ly);    // :110, :113
   const double2 a_ref = cmul_rn(cconj(ur_ref), cconj(er_ref));
   const double2 a_trn = cmul_rn(cconj(ur_trn), cconj(er_trn));
   bool wood = false;
@@ -190,7 +190,7 @@ __global__ void wavevec_kernel(const SourceDev* __restrict__ srcs, double lx, do
 __global__ void assemble_pq_kernel(int N, const double2* __restrict__ erc,
                                    const double2* __restrict__ urc,
                                    const double2* __restrict__ einv,
-                                   const double2* __restrict__ uinv,
+                                   const double2* __restrict__ uinv, long long s_item,
                                    const double2* __restrict__ Kxg,
                                    const double2* __restrict__ Kyg, double2* __restrict__ P,
                                    double2* __restrict__ Qm) {
@@ -203,7 +203,7 @@ __global__ void assemble_pq_kernel(int N, const double2* __restrict__ erc,
   const int ii = i - bi * N, jj = j - bj * N;
   const double2* Kx = Kxg + (long long)b * N;
   const double2* Ky = Kyg + (long long)b * N;
-  const long long o = (long long)jj * N + ii;
+  const long long o = (long long)b * s_item + (long long)jj * N + ii;
   const double2 ei = einv[o], ui = uinv[o], ec = erc[o], uc = urc[o];
   double2 p, q;
   if (!bi && !bj) {
@@ -226,11 +226,13 @@ __global__ void assemble_pq_kernel(int N, const double2* __restrict__ erc,
 
 __global__ void layer_modes_kernel(int n, const double2* __restrict__ lam2,
                                    const double2* __restrict__ kinc, double t,
+                                   const double* __restrict__ t_item, int t_stride,
                                    double2* __restrict__ lam, double2* __restrict__ ilam,
                                    double2* __restrict__ X) {
   const int b = blockIdx.y;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
+  if (t_item) t = t_item[(long long)b * t_stride];
   const long long o = (long long)b * n + j;
   const double k0 = kinc[(long long)b * 4 + 3].x;
   const double2 l = usqrt(lam2[o]);                       // :317
@@ -325,12 +327,18 @@ __device__ __forceinline__ C22 gap_v0(const double2* V0, int N, int i) {
 // of rcwa.cpp:262-351 is 2x2-block diagonal over the (i, i+N) pairs and
 // Omega^2 = (kx^2 + ky^2 - mu eps) I.  The eigenbasis W = I is used; S is
 // invariant to the choice of basis inside the degenerate pairs.
-__global__ void uniform_layer_kernel(int N, double2 eps, double2 mu, double t, WaveVecs w,
+__global__ void uniform_layer_kernel(int N, double2 eps, double2 mu, double t,
+                                     const double2* __restrict__ eps_item,
+                                     const double2* __restrict__ mu_item,
+                                     const double* __restrict__ t_item, int stride, WaveVecs w,
                                      double2* __restrict__ S11g, double2* __restrict__ S12g,
                                      long long sS, int bd) {
   const int b = blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
+  if (eps_item) eps = eps_item[(long long)b * stride];
+  if (mu_item) mu = mu_item[(long long)b * stride];
+  if (t_item) t = t_item[(long long)b * stride];
   const int n = 2 * N;
   const long long o = (long long)b * N + i;
   const double2 kx = w.Kx[o], ky = w.Ky[o];
@@ -652,10 +660,10 @@ int convmat(cudaStream_t s, const double2* grids, int nl, int nx, int ny, const 
   return RCWA_OK;
 }
 
-int wave_vectors(cudaStream_t s, const SourceDev* src_dev, int B, double lx, double ly,
-                 const ModeDims& d, double2 er_ref, double2 ur_ref, double2 er_trn,
-                 double2 ur_trn, const WaveVecs& w, uint32_t* status) {
-  wavevec_kernel<<<B, 256, 0, s>>>(src_dev, lx, ly, d.nxh, d.nyh, d.Q, d.N, er_ref, ur_ref, er_trn,
+int wave_vectors(cudaStream_t s, const SourceDev* src_dev, int B, const ModeDims& d,
+                 double2 er_ref, double2 ur_ref, double2 er_trn, double2 ur_trn,
+                 const WaveVecs& w, uint32_t* status) {
+  wavevec_kernel<<<B, 256, 0, s>>>(src_dev, d.nxh, d.nyh, d.Q, d.N, er_ref, ur_ref, er_trn,
                                    ur_trn, w, status);
   count_launch();
   RCWA_LAUNCH_CHECK();
@@ -663,19 +671,20 @@ int wave_vectors(cudaStream_t s, const SourceDev* src_dev, int B, double lx, dou
 }
 
 int assemble_pq(cudaStream_t s, int B, const ModeDims& d, const double2* erc, const double2* urc,
-                const double2* einv, const double2* uinv, const WaveVecs& w, double2* P,
-                double2* Qm) {
+                const double2* einv, const double2* uinv, long long s_item, const WaveVecs& w,
+                double2* P, double2* Qm) {
   const long long nn = (long long)d.n * d.n;
-  assemble_pq_kernel<<<dim3(cdiv_up(nn, 256), B), 256, 0, s>>>(d.N, erc, urc, einv, uinv, w.Kx,
-                                                                w.Ky, P, Qm);
+  assemble_pq_kernel<<<dim3(cdiv_up(nn, 256), B), 256, 0, s>>>(d.N, erc, urc, einv, uinv, s_item,
+                                                                w.Kx, w.Ky, P, Qm);
   count_launch();
   RCWA_LAUNCH_CHECK();
   return RCWA_OK;
 }
 
 int layer_modes(cudaStream_t s, int B, int n, const double2* lam2, const double2* kinc, double t,
-                double2* lam, double2* ilam, double2* X) {
-  layer_modes_kernel<<<dim3(cdiv_up(n, 256), B), 256, 0, s>>>(n, lam2, kinc, t, lam, ilam, X);
+                const double* t_item, int t_stride, double2* lam, double2* ilam, double2* X) {
+  layer_modes_kernel<<<dim3(cdiv_up(n, 256), B), 256, 0, s>>>(n, lam2, kinc, t, t_item, t_stride,
+                                                               lam, ilam, X);
   count_launch();
   RCWA_LAUNCH_CHECK();
   return RCWA_OK;
@@ -691,9 +700,10 @@ int assemble_ab(cudaStream_t s, int B, const ModeDims& d, const double2* Wi, lon
 }
 
 int uniform_layer(cudaStream_t s, int B, const ModeDims& d, double2 eps, double2 mu, double t,
-                  const WaveVecs& w, double2* S11, double2* S12, long long sS, int bd) {
-  uniform_layer_kernel<<<dim3(cdiv_up(d.N, 128), B), 128, 0, s>>>(d.N, eps, mu, t, w, S11, S12, sS,
-                                                                   bd);
+                  const double2* eps_item, const double2* mu_item, const double* t_item,
+                  int stride, const WaveVecs& w, double2* S11, double2* S12, long long sS, int bd) {
+  uniform_layer_kernel<<<dim3(cdiv_up(d.N, 128), B), 128, 0, s>>>(d.N, eps, mu, t, eps_item, mu_item,
+                                                                   t_item, stride, w, S11, S12, sS, bd);
   count_launch();
   RCWA_LAUNCH_CHECK();
   return RCWA_OK;

@@ -369,18 +369,19 @@ int fold_status(cudaStream_t s, uint32_t* dst, const uint32_t* scratch, int B, i
 
 // S-matrix of one patterned layer (rcwa.cpp:254-352) for the chunk.
 // Output: S11 at augD[1] (stride 3n^2) and S12 in s2.
-int patterned_layer(rcwa_context* ctx, const rcwa_geometry* g, int l, Plan& pl,
-                    uint32_t* status) {
+int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, uint32_t* status) {
   cudaStream_t s = ctx->stream;
-  const ModeDims& d = g->d;
+  const ModeDims& d = g.d;
   const int B = pl.B, n = d.n;
   const long long nn = (long long)n * n, NN = (long long)d.N * d.N;
   const long long s2 = 2 * nn, s3 = 3 * nn;
   const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
   int rc;
   // P_i, Q_i (:262-286)
-  if ((rc = assemble_pq(s, B, d, g->erc + l * NN, g->urc + l * NN, g->einv + l * NN,
-                        g->uinv + l * NN, pl.wv, pl.s0, pl.s1)))
+  (void)NN;
+  const long long lo = l * g.s_layer;
+  if ((rc = assemble_pq(s, B, d, g.erc + lo, g.urc + lo, g.einv + lo, g.uinv + lo, g.s_item, pl.wv,
+                        pl.s0, pl.s1)))
     return rc;
   // Omega^2 = P Q (:288)
   ZGemm gm;
@@ -394,7 +395,9 @@ int patterned_layer(rcwa_context* ctx, const rcwa_geometry* g, int l, Plan& pl,
   if ((rc = zeig(s, n, B, pl.s2, n, nn, pl.augWV, s2, pl.lam2, n, pl.st, pl.eigws))) return rc;
   if ((rc = fold_status(s, status, pl.st, B, 1))) return rc;
   // lambda, 1/lambda, X (:317, :339)
-  if ((rc = layer_modes(s, B, n, pl.lam2, pl.wv.kinc, g->t[l], pl.lam, pl.ilam, pl.X))) return rc;
+  if ((rc = layer_modes(s, B, n, pl.lam2, pl.wv.kinc, g.t ? g.t[l] : 0.0, g.t_item ? g.t_item + l : nullptr,
+                        g.nl, pl.lam, pl.ilam, pl.X)))
+    return rc;
   // V = Q W lambda^-1 (:326-330) into the first half of [V | I]
   double2* augV = pl.augWV + (long long)B * s2;
   gm = ZGemm();
@@ -589,10 +592,34 @@ int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, c
 
 size_t sweep_bytes_per_source(const ModeDims& d) { return plan_bytes(d, 1); }
 
-static int sweep_chunk(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* sources,
-                       int B, double* R, double* T, double* tot, uint32_t* status) {
+// The layer set of one geometry, shared by every solve of a sweep.
+Layers layers_of(const rcwa_geometry* g) {
+  Layers G;
+  G.d = g->d;
+  G.nl = g->nl;
+  G.er_ref = g->er_ref;
+  G.ur_ref = g->ur_ref;
+  G.er_trn = g->er_trn;
+  G.ur_trn = g->ur_trn;
+  G.uniform = g->uniform.data();
+  G.t = g->t.data();
+  G.ueps = g->ueps.data();
+  G.umu = g->umu.data();
+  G.erc = g->erc;
+  G.urc = g->urc;
+  G.einv = g->einv;
+  G.uinv = g->uinv;
+  G.s_layer = (long long)g->d.N * g->d.N;
+  G.s_item = 0;
+  return G;
+}
+
+// One chunk of B solves on the layer set g; hsrc: host [B] sources with
+// their lattice periods.
+int sweep_chunk_layers(rcwa_context* ctx, const Layers& g, const SourceDev* hsrc, int B, double* R,
+                       double* T, double* tot, uint32_t* status) {
   cudaStream_t s = ctx->stream;
-  const ModeDims& d = g->d;
+  const ModeDims& d = g.d;
   const int n = d.n;
   const long long nn = (long long)n * n, s3 = 3 * nn;
   Plan pl;
@@ -602,13 +629,11 @@ static int sweep_chunk(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_sou
   if ((rc = ctx_pinned(ctx, (size_t)B * sizeof(SourceDev)))) return rc;
   SourceDev* hs = (SourceDev*)ctx->pinned;
   RCWA_CUDA_TRY(cudaStreamSynchronize(s));  // staging buffer reuse
-  for (int b = 0; b < B; ++b)
-    hs[b] = SourceDev{sources[b].lambda0, sources[b].theta, sources[b].phi, sources[b].pte, sources[b].ptm};
+  std::memcpy(hs, hsrc, B * sizeof(SourceDev));
   RCWA_CUDA_TRY(cudaMemcpyAsync(pl.src, hs, B * sizeof(SourceDev), cudaMemcpyHostToDevice, s));
   RCWA_CUDA_TRY(cudaMemsetAsync(status, 0, B * sizeof(uint32_t), s));
   // wave vectors + gap (main.cpp:140-141)
-  if ((rc = wave_vectors(s, pl.src, B, g->lx, g->ly, d, g->er_ref, g->ur_ref, g->er_trn, g->ur_trn,
-                         pl.wv, status)))
+  if ((rc = wave_vectors(s, pl.src, B, d, g.er_ref, g.ur_ref, g.er_trn, g.ur_trn, pl.wv, status)))
     return rc;
   // device S-matrix (main.cpp:143-164)
   SMat dev;
@@ -618,10 +643,12 @@ static int sweep_chunk(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_sou
   }
   double2* tmp = pl.tmp;
   const long long sL = 8LL * d.N;     // BD uniform layer: S11 (4N) + S12 (4N) per source
-  for (int l = 0; l < g->nl; ++l) {
-    if (g->uniform[l]) {
-      if ((rc = uniform_layer(s, B, d, g->ueps[l], g->umu[l], g->t[l], pl.wv, pl.lbd, pl.lbd + 4 * d.N,
-                              sL, 1)))
+  for (int l = 0; l < g.nl; ++l) {
+    if (g.uniform[l]) {
+      if ((rc = uniform_layer(s, B, d, g.ueps ? g.ueps[l] : make_double2(1, 0),
+                              g.umu ? g.umu[l] : make_double2(1, 0), g.t ? g.t[l] : 0.0,
+                              g.ueps_item ? g.ueps_item + l : nullptr, g.umu_item ? g.umu_item + l : nullptr,
+                              g.t_item ? g.t_item + l : nullptr, g.nl, pl.wv, pl.lbd, pl.lbd + 4 * d.N, sL, 1)))
         return rc;
       if (l == 0) {
         // S_init (x) S_layer == S_layer exactly (S11 = S22 = 0, S12 = S21 = I)
@@ -651,7 +678,7 @@ static int sweep_chunk(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_sou
       if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
     }
   }
-  if (g->nl == 0) {
+  if (g.nl == 0) {
     for (int k = 0; k < 4; ++k) {
       if ((rc = fill_zero(s, dev.p[k], (size_t)B * nn))) return rc;
     }
@@ -663,10 +690,10 @@ static int sweep_chunk(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_sou
   const long long sP = 32LL * d.N;
   double2* Rbd = pl.pbd;
   double2* Tbd = pl.pbd + 16 * d.N;
-  if ((rc = port_smatrix(s, B, d, 0, g->er_ref, g->ur_ref, pl.wv, Rbd, Rbd + 4 * d.N, Rbd + 8 * d.N,
+  if ((rc = port_smatrix(s, B, d, 0, g.er_ref, g.ur_ref, pl.wv, Rbd, Rbd + 4 * d.N, Rbd + 8 * d.N,
                          Rbd + 12 * d.N, sP, 1)))
     return rc;
-  if ((rc = port_smatrix(s, B, d, 1, g->er_trn, g->ur_trn, pl.wv, Tbd, Tbd + 4 * d.N, Tbd + 8 * d.N,
+  if ((rc = port_smatrix(s, B, d, 1, g.er_trn, g.ur_trn, pl.wv, Tbd, Tbd + 4 * d.N, Tbd + 8 * d.N,
                          Tbd + 12 * d.N, sP, 1)))
     return rc;
   double2* S11E = pl.s2;
@@ -675,7 +702,7 @@ static int sweep_chunk(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_sou
                            pl.s0, pl.s1, pl.piv, pl.st, status)))
     return rc;
   // efficiencies (main.cpp:182-191)
-  return efficiencies(s, B, d, pl.src, g->ur_ref, g->ur_trn, pl.wv, S11E, S21E, 2LL * n, 1, R, T,
+  return efficiencies(s, B, d, pl.src, g.ur_ref, g.ur_trn, pl.wv, S11E, S21E, 2LL * n, 1, R, T,
                       tot, status);
 }
 
@@ -711,11 +738,16 @@ int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* s
   const size_t per = plan_bytes(d, 1);
   int chunk = (int)std::max<size_t>(1, budget / per);
   chunk = std::min(chunk, B);
+  const Layers G = layers_of(g);
+  std::vector<SourceDev> hs(chunk);
   for (int b0 = 0; b0 < B; b0 += chunk) {
     const int bc = std::min(chunk, B - b0);
     const long long N = d.N;
-    int rc = sweep_chunk(ctx, g, sources + b0, bc, R + b0 * N, T + b0 * N, tot + 2LL * b0,
-                         status + b0);
+    for (int b = 0; b < bc; ++b) {
+      const rcwa_source& q = sources[b0 + b];
+      hs[b] = SourceDev{q.lambda0, q.theta, q.phi, q.pte, q.ptm, g->lx, g->ly};
+    }
+    int rc = sweep_chunk_layers(ctx, G, hs.data(), bc, R + b0 * N, T + b0 * N, tot + 2LL * b0, status + b0);
     if (rc) return rc;
   }
   if (tc_err) {
@@ -781,10 +813,10 @@ int step_wave_vectors(rcwa_context* ctx, double lx, double ly, const rcwa_source
   w.kinc = (double2*)a.take(4 * 16);
   SourceDev* ds = (SourceDev*)a.take(sizeof(SourceDev));
   uint32_t* st = (uint32_t*)a.take(4);
-  SourceDev hs{src->lambda0, src->theta, src->phi, src->pte, src->ptm};
+  SourceDev hs{src->lambda0, src->theta, src->phi, src->pte, src->ptm, lx, ly};
   if ((rc = h2d(ctx, ds, &hs, sizeof(hs)))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 4, ctx->stream));
-  if ((rc = wave_vectors(ctx->stream, ds, 1, lx, ly, d, c2(p->er_ref), c2(p->ur_ref), c2(p->er_trn),
+  if ((rc = wave_vectors(ctx->stream, ds, 1, d, c2(p->er_ref), c2(p->ur_ref), c2(p->er_trn),
                          c2(p->ur_trn), w, st)))
     return rc;
   if ((rc = d2h(ctx, Kx, w.Kx, N * 16)) || (rc = d2h(ctx, Ky, w.Ky, N * 16)) ||
@@ -846,7 +878,7 @@ int step_smatrix_layer(rcwa_context* ctx, int N, const double2* erc, const doubl
   if ((rc = h2d(ctx, pl.wv.Kx, Kx, (size_t)N * 16)) || (rc = h2d(ctx, pl.wv.Ky, Ky, (size_t)N * 16)) ||
       (rc = h2d(ctx, pl.wv.V0, V0d, (size_t)4 * N * 16)) || (rc = h2d(ctx, pl.wv.kinc, kinc, sizeof(kinc))))
     return rc;
-  if ((rc = patterned_layer(ctx, &g, 0, pl, dst))) return rc;
+  if ((rc = patterned_layer(ctx, layers_of(&g), 0, pl, dst))) return rc;
   if ((rc = d2h(ctx, S11, pl.augD + nn, nn * 16)) || (rc = d2h(ctx, S12, pl.augD + 2 * nn, nn * 16)))
     return rc;
   uint32_t hs[2] = {0, 0};

@@ -46,6 +46,35 @@ namespace rcwa {
 int ctx_reserve(rcwa_context* ctx, size_t bytes);
 int ctx_pinned(rcwa_context* ctx, size_t bytes);
 
+// The stack as one solve chunk sees it.  A sweep shares one geometry between
+// all its solves (s_item = 0, per-layer scalars on the host); a batch of
+// unrelated stacks of equal shape gives every solve its own matrices (item b,
+// layer l at b * s_item + l * s_layer) and per-item scalars in device arrays
+// [B][nl] (t_item, ueps_item, umu_item).
+struct Layers {
+  ModeDims d{};
+  int nl = 0;
+  double2 er_ref{}, ur_ref{}, er_trn{}, ur_trn{};
+  const char* uniform = nullptr;   // host [nl]
+  const double* t = nullptr;       // host [nl], shared
+  const double2* ueps = nullptr;   // host [nl], shared
+  const double2* umu = nullptr;
+  const double2 *erc = nullptr, *urc = nullptr, *einv = nullptr, *uinv = nullptr;
+  long long s_layer = 0, s_item = 0;
+  const double* t_item = nullptr;
+  const double2* ueps_item = nullptr;
+  const double2* umu_item = nullptr;
+};
+Layers layers_of(const rcwa_geometry* g);
+// One chunk of B solves (device outputs R/T [B][N], tot [B][2], status [B]);
+// hsrc: host array of the B sources with their lattice periods.
+int sweep_chunk_layers(rcwa_context* ctx, const Layers& g, const SourceDev* hsrc, int B, double* R,
+                       double* T, double* tot, uint32_t* status);
+// n unrelated problems, grouped by shape into batched solves (batch.cu);
+// max_group > 0 caps the solves per batched launch sequence.
+int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_source* sources,
+                const rcwa_params* params, int precision, int max_group, rcwa_result* out);
+
 // Build convolution matrices and their inverses.  grids_er/ur are device
 // pointers ([nl][ny][nx]) when on_device, host pointers otherwise.
 int geometry_build(rcwa_context* ctx, rcwa_geometry* g, const rcwa_stack* st,

@@ -102,6 +102,15 @@ _SIGS = {
     "rcwa_eig_noalloc": ([C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_lu_solve": ([_VP, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_gemm": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, C.c_int], C.c_int),
+    "rcwa_solve_batch": ([_VP, C.c_int, C.POINTER(CStack), C.POINTER(CSource), C.POINTER(CParams),
+                          C.c_int, C.POINTER(CResult)], C.c_int),
+    "rcwa_server_create": ([C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_VP)], C.c_int),
+    "rcwa_server_submit": ([_VP, C.POINTER(CStack), C.POINTER(CSource), C.POINTER(CParams),
+                            C.POINTER(C.c_uint64)], C.c_int),
+    "rcwa_server_poll": ([_VP, C.c_uint64, C.c_int, C.POINTER(CResult), C.POINTER(C.c_int)], C.c_int),
+    "rcwa_server_stats": ([_VP, C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.POINTER(C.c_double)],
+                          C.c_int),
+    "rcwa_server_destroy": ([_VP], C.c_int),
 }
 
 _lib = None
@@ -409,3 +418,90 @@ class Context:
         _check(self.lib.rcwa_gemm(self.h, m, n, k, b, _ptr(Af), _ptr(Bf), _ptr(Cf), precision))
         Cm = Cf.transpose(0, 2, 1)
         return Cm[0] if single else Cm
+
+    # ---- batches of unrelated problems --------------------------------------
+    def solve_batch(self, problems: Sequence[Problem], precision: int = PREC_FP64,
+                    source_index: Optional[Sequence[int]] = None):
+        """``rcwa_solve_batch``: problem i is (problems[i].stack,
+        problems[i].sources[source_index[i] or 0], problems[i].params).
+        Returns (R, T, R_tot, T_tot, status) as lists ([Q, P] arrays)."""
+        n = len(problems)
+        if n == 0:
+            return [], [], np.zeros(0), np.zeros(0), np.zeros(0, np.uint32)
+        keep = []
+        stacks = (CStack * n)()
+        srcs = (CSource * n)()
+        prms = (CParams * n)()
+        res = (CResult * n)()
+        outR, outT = [], []
+        for i, pb in enumerate(problems):
+            st = pb.stack
+            er, ur = _c128(st.er), _c128(st.ur)
+            t = np.ascontiguousarray(st.t, dtype=np.float64)
+            keep += [er, ur, t]
+            stacks[i] = CStack(st.Nx, st.Ny, st.num_layers, st.Lx, st.Ly, _ptr(er), _ptr(ur), _ptr(t))
+            k = 0 if source_index is None else int(source_index[i])
+            srcs[i] = c_source(pb.sources[k])
+            prms[i] = c_params(pb.params)
+            P = 2 * pb.params.nx_harmonics + 1
+            Q = 2 * pb.params.ny_harmonics + 1
+            R = np.zeros(P * Q)
+            T = np.zeros(P * Q)
+            outR.append(R)
+            outT.append(T)
+            res[i].R = R.ctypes.data
+            res[i].T = T.ctypes.data
+        _check(self.lib.rcwa_solve_batch(self.h, n, stacks, srcs, prms, precision, res),
+               allow_numeric=True)
+        del keep
+        Rs, Ts = [], []
+        for pb, R, T in zip(problems, outR, outT):
+            P = 2 * pb.params.nx_harmonics + 1
+            Q = 2 * pb.params.ny_harmonics + 1
+            Rs.append(R.reshape(P, Q).T)
+            Ts.append(T.reshape(P, Q).T)
+        return (Rs, Ts, np.array([r.R_tot for r in res]), np.array([r.T_tot for r in res]),
+                np.array([r.status for r in res], dtype=np.uint32))
+
+
+class Server:
+    """``rcwa_server_*``: a serving loop with continuous batching on one GPU."""
+
+    def __init__(self, device: int = 0, max_batch: int = 256, max_queue: int = 100000,
+                 precision: int = PREC_FP64):
+        self.lib = load()
+        self.h = C.c_void_p()
+        _check(self.lib.rcwa_server_create(device, max_batch, max_queue, precision, C.byref(self.h)))
+
+    def submit(self, pb: Problem, source_index: int = 0) -> int:
+        st = pb.stack
+        er, ur = _c128(st.er), _c128(st.ur)
+        t = np.ascontiguousarray(st.t, dtype=np.float64)
+        cst = CStack(st.Nx, st.Ny, st.num_layers, st.Lx, st.Ly, _ptr(er), _ptr(ur), _ptr(t))
+        tk = C.c_uint64()
+        _check(self.lib.rcwa_server_submit(self.h, C.byref(cst), C.byref(c_source(pb.sources[source_index])),
+                                           C.byref(c_params(pb.params)), C.byref(tk)))
+        return int(tk.value)
+
+    def poll(self, ticket: int, pb: Problem, wait: bool = True):
+        """(done, R [Q, P], T [Q, P], R_tot, T_tot, status) of one request."""
+        P = 2 * pb.params.nx_harmonics + 1
+        Q = 2 * pb.params.ny_harmonics + 1
+        R = np.zeros(P * Q)
+        T = np.zeros(P * Q)
+        res = CResult(R.ctypes.data, T.ctypes.data, 0.0, 0.0, 0)
+        done = C.c_int(0)
+        _check(self.lib.rcwa_server_poll(self.h, ticket, 1 if wait else 0, C.byref(res), C.byref(done)),
+               allow_numeric=True)
+        return (bool(done.value), R.reshape(P, Q).T, T.reshape(P, Q).T, res.R_tot, res.T_tot,
+                int(res.status))
+
+    def stats(self):
+        n, p50, p99 = C.c_uint64(), C.c_double(), C.c_double()
+        _check(self.lib.rcwa_server_stats(self.h, C.byref(n), C.byref(p50), C.byref(p99)))
+        return int(n.value), float(p50.value), float(p99.value)
+
+    def close(self):
+        if self.h:
+            self.lib.rcwa_server_destroy(self.h)
+            self.h = C.c_void_p()
