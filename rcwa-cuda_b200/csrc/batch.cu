@@ -290,7 +290,9 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
     d.Q = 2 * d.nyh + 1;
     d.N = d.P * d.Q;
     d.n = 2 * d.N;
-    const size_t per = sweep_bytes_per_source(d) + geometry_bytes_per_item(d, k.nl, k.nx, k.ny);
+    int np = 0;
+    for (int l = 0; l < k.nl; ++l) np += k.uniform[l] ? 0 : 1;
+    const size_t per = sweep_bytes_per_source(d, np) + geometry_bytes_per_item(d, k.nl, k.nx, k.ny);
     int chunk = (int)std::max<size_t>(1, budget / per);
     if (max_group > 0) chunk = std::min(chunk, max_group);
     const std::vector<int>& m = members[g];

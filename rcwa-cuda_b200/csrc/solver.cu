@@ -283,7 +283,12 @@ struct Plan {
   double2* augA;    // [B] x 2n^2
   double2* augD;    // [B] x 3n^2
   double2* augFG;   // [2B] x 3n^2
-  double2* eigws;   // zeig workspace
+  double2* eigws;   // zeig workspace for np * B matrices
+  int np;           // patterned layers the plan holds eigen-decompositions for
+  double2* OmA;     // [np][B] n x n: Omega^2 (destroyed by the eigensolver)
+  double2* Wst;     // [np][B] n x n: eigenvectors W
+  double2* L2st;    // [np][B][n]: eigenvalues lambda^2
+  uint32_t* est;    // [np][B] eigensolver status
   double2* lam2;    // [B][n]
   double2* lam;     // [B][n]
   double2* ilam;    // [B][n]
@@ -296,11 +301,13 @@ struct Plan {
 
 constexpr int kBlocksPerSource = 4 + 1 + 4 + 4 + 2 + 3 + 6;  // SD,tmp,s0-3,augWV,augA,augD,augFG
 
-size_t plan_bytes(const ModeDims& d, int B) {
+size_t plan_bytes(const ModeDims& d, int B, int np) {
   const size_t nn = (size_t)d.n * d.n;
+  const int ne = np > 0 ? np : 1;
   size_t b = (size_t)B * kBlocksPerSource * nn * sizeof(double2);
   b += (size_t)B * 40 * d.N * sizeof(double2);                // pbd, lbd
-  b += zeig_workspace_bytes(d.n, B);
+  b += zeig_workspace_bytes(d.n, ne * B);
+  b += (size_t)ne * B * (2 * nn + d.n) * sizeof(double2) + (size_t)ne * B * sizeof(uint32_t) + 4 * 256;
   b += (size_t)B * 4 * d.n * sizeof(double2);                 // lam2, lam, ilam, X
   b += (size_t)B * (4 * d.N + 4 * d.N + 4) * sizeof(double2); // Kx Ky Kzr Kzt, V0, kinc
   b += (size_t)B * sizeof(SourceDev) + (size_t)3 * B * sizeof(uint32_t);
@@ -309,8 +316,8 @@ size_t plan_bytes(const ModeDims& d, int B) {
   return (b + 255) & ~(size_t)255;  // callers place further buffers right after the plan
 }
 
-int plan_take(rcwa_context* ctx, const ModeDims& d, int B, Plan& pl) {
-  int rc = ctx_reserve(ctx, plan_bytes(d, B));
+int plan_take(rcwa_context* ctx, const ModeDims& d, int B, int np, Plan& pl) {
+  int rc = ctx_reserve(ctx, plan_bytes(d, B, np));
   if (rc) return rc;
   char* w = (char*)ctx->ws;
   auto take = [&](size_t bytes) {
@@ -335,7 +342,13 @@ int plan_take(rcwa_context* ctx, const ModeDims& d, int B, Plan& pl) {
   pl.augA = (double2*)take(2 * blk);
   pl.augD = (double2*)take(3 * blk);
   pl.augFG = (double2*)take(6 * blk);
-  pl.eigws = (double2*)take(zeig_workspace_bytes(d.n, B));
+  const int ne = np > 0 ? np : 1;
+  pl.np = ne;
+  pl.eigws = (double2*)take(zeig_workspace_bytes(d.n, ne * B));
+  pl.OmA = (double2*)take((size_t)ne * blk);
+  pl.Wst = (double2*)take((size_t)ne * blk);
+  pl.L2st = (double2*)take((size_t)ne * B * d.n * sizeof(double2));
+  pl.est = (uint32_t*)take((size_t)ne * B * sizeof(uint32_t));
   pl.lam2 = (double2*)take((size_t)B * d.n * sizeof(double2));
   pl.lam = (double2*)take((size_t)B * d.n * sizeof(double2));
   pl.ilam = (double2*)take((size_t)B * d.n * sizeof(double2));
@@ -369,33 +382,71 @@ int fold_status(cudaStream_t s, uint32_t* dst, const uint32_t* scratch, int B, i
 
 // S-matrix of one patterned layer (rcwa.cpp:254-352) for the chunk.
 // Output: S11 at augD[1] (stride 3n^2) and S12 in s2.
-int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, uint32_t* status) {
+// Omega^2 = P Q of patterned layer l (rcwa.cpp:262-288) for the chunk -> out
+// (packed n x n per source).
+int layer_omega2(rcwa_context* ctx, const Layers& g, int l, Plan& pl, double2* out) {
   cudaStream_t s = ctx->stream;
   const ModeDims& d = g.d;
   const int B = pl.B, n = d.n;
-  const long long nn = (long long)n * n, NN = (long long)d.N * d.N;
-  const long long s2 = 2 * nn, s3 = 3 * nn;
-  const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
+  const long long nn = (long long)n * n;
   int rc;
-  // P_i, Q_i (:262-286)
-  (void)NN;
   const long long lo = l * g.s_layer;
   if ((rc = assemble_pq(s, B, d, g.erc + lo, g.urc + lo, g.einv + lo, g.uinv + lo, g.s_item, pl.wv,
                         pl.s0, pl.s1)))
     return rc;
-  // Omega^2 = P Q (:288)
   ZGemm gm;
   gm.m = n; gm.n = n; gm.k = n; gm.batch = B;
   gm.A = pl.s0; gm.lda = n; gm.sA = nn;
   gm.B = pl.s1; gm.ldb = n; gm.sB = nn;
-  gm.C = pl.s2; gm.ldc = n; gm.sC = nn;
-  if ((rc = zgemm(s, gm))) return rc;
-  // eig (:298-306): W written straight into the first half of [W | I]
-  RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zeig(s, n, B, pl.s2, n, nn, pl.augWV, s2, pl.lam2, n, pl.st, pl.eigws))) return rc;
-  if ((rc = fold_status(s, status, pl.st, B, 1))) return rc;
+  gm.C = out; gm.ldc = n; gm.sC = nn;
+  return zgemm(s, gm);
+}
+
+// Eigen-decompositions (rcwa.cpp:298-306) of the patterned layers `pat` of the
+// chunk, all in ONE batched eigensolver call of np * B matrices (more
+// independent matrices per launch fill the SMs better than one launch per
+// layer).  Layer pat[k] of source b: W at pl.Wst + (k B + b) n^2, lambda^2 at
+// pl.L2st + (k B + b) n.
+int eig_layers(rcwa_context* ctx, const Layers& g, const std::vector<int>& pat, Plan& pl,
+               uint32_t* status) {
+  cudaStream_t s = ctx->stream;
+  const int B = pl.B, n = g.d.n, np = (int)pat.size();
+  if (np == 0) return RCWA_OK;
+  if (np > pl.np) {
+    set_last_error("internal: plan sized for %d patterned layers, %d needed", pl.np, np);
+    return RCWA_ERR_INVALID;
+  }
+  const long long nn = (long long)n * n;
+  int rc;
+  for (int k = 0; k < np; ++k)
+    if ((rc = layer_omega2(ctx, g, pat[k], pl, pl.OmA + (size_t)k * B * nn))) return rc;
+  RCWA_CUDA_TRY(cudaMemsetAsync(pl.est, 0, (size_t)np * B * sizeof(uint32_t), s));
+  if ((rc = zeig(s, n, np * B, pl.OmA, n, nn, pl.Wst, nn, pl.L2st, n, pl.est, pl.eigws))) return rc;
+  return fold_status(s, status, pl.est, B, np);
+}
+
+// S-matrix of one patterned layer (rcwa.cpp:254-352) for the chunk, from its
+// eigen-decomposition Wl (packed n x n per source) and lam2l (n per source).
+// Output: S11 at augD[1] (stride 3n^2) and S12 at augD[2].
+int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const double2* Wl,
+                    const double2* lam2l, uint32_t* status) {
+  cudaStream_t s = ctx->stream;
+  const ModeDims& d = g.d;
+  const int B = pl.B, n = d.n;
+  const long long nn = (long long)n * n;
+  const long long s2 = 2 * nn, s3 = 3 * nn;
+  const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
+  int rc;
+  // Q_i (:280-286) again (P is not needed past Omega^2)
+  const long long lo = l * g.s_layer;
+  if ((rc = assemble_pq(s, B, d, g.erc + lo, g.urc + lo, g.einv + lo, g.uinv + lo, g.s_item, pl.wv,
+                        pl.s0, pl.s1)))
+    return rc;
+  // W into the first half of [W | I]
+  if ((rc = copy_blocks(s, pl.augWV, s2, Wl, nn, nn, B))) return rc;
+  ZGemm gm;
   // lambda, 1/lambda, X (:317, :339)
-  if ((rc = layer_modes(s, B, n, pl.lam2, pl.wv.kinc, g.t ? g.t[l] : 0.0, g.t_item ? g.t_item + l : nullptr,
+  if ((rc = layer_modes(s, B, n, lam2l, pl.wv.kinc, g.t ? g.t[l] : 0.0, g.t_item ? g.t_item + l : nullptr,
                         g.nl, pl.lam, pl.ilam, pl.X)))
     return rc;
   // V = Q W lambda^-1 (:326-330) into the first half of [V | I]
@@ -590,7 +641,7 @@ int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, c
 
 }  // namespace
 
-size_t sweep_bytes_per_source(const ModeDims& d) { return plan_bytes(d, 1); }
+size_t sweep_bytes_per_source(const ModeDims& d, int np) { return plan_bytes(d, 1, np); }
 
 // The layer set of one geometry, shared by every solve of a sweep.
 Layers layers_of(const rcwa_geometry* g) {
@@ -622,8 +673,10 @@ int sweep_chunk_layers(rcwa_context* ctx, const Layers& g, const SourceDev* hsrc
   const ModeDims& d = g.d;
   const int n = d.n;
   const long long nn = (long long)n * n, s3 = 3 * nn;
+  int np = 0;
+  for (int l = 0; l < g.nl; ++l) np += g.uniform[l] ? 0 : 1;
   Plan pl;
-  int rc = plan_take(ctx, d, B, pl);
+  int rc = plan_take(ctx, d, B, np, pl);
   if (rc) return rc;
   // sources -> device (through the pinned staging buffer)
   if ((rc = ctx_pinned(ctx, (size_t)B * sizeof(SourceDev)))) return rc;
@@ -643,6 +696,13 @@ int sweep_chunk_layers(rcwa_context* ctx, const Layers& g, const SourceDev* hsrc
   }
   double2* tmp = pl.tmp;
   const long long sL = 8LL * d.N;     // BD uniform layer: S11 (4N) + S12 (4N) per source
+  std::vector<int> pat, slot(g.nl, -1);
+  for (int l = 0; l < g.nl; ++l)
+    if (!g.uniform[l]) {
+      slot[l] = (int)pat.size();
+      pat.push_back(l);
+    }
+  if ((rc = eig_layers(ctx, g, pat, pl, status))) return rc;
   for (int l = 0; l < g.nl; ++l) {
     if (g.uniform[l]) {
       if ((rc = uniform_layer(s, B, d, g.ueps ? g.ueps[l] : make_double2(1, 0),
@@ -663,7 +723,8 @@ int sweep_chunk_layers(rcwa_context* ctx, const Layers& g, const SourceDev* hsrc
       }
       continue;
     }
-    if ((rc = patterned_layer(ctx, g, l, pl, status))) return rc;
+    const size_t k = (size_t)slot[l];
+    if ((rc = patterned_layer(ctx, g, l, pl, pl.Wst + k * B * nn, pl.L2st + k * B * n, status))) return rc;
     SMat lay;
     lay.p[0] = pl.augD + nn; lay.s[0] = s3;      // S11 = D^-1 R1
     lay.p[1] = pl.augD + 2 * nn; lay.s[1] = s3;  // S12 = D^-1 X R2
@@ -735,7 +796,9 @@ int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* s
     RCWA_CUDA_TRY(cudaMemGetInfo(&fr, &totm));
     budget = (size_t)((fr + ctx->ws_bytes) * 0.6);
   }
-  const size_t per = plan_bytes(d, 1);
+  int np = 0;
+  for (int l = 0; l < g->nl; ++l) np += g->uniform[l] ? 0 : 1;
+  const size_t per = plan_bytes(d, 1, np);
   int chunk = (int)std::max<size_t>(1, budget / per);
   chunk = std::min(chunk, B);
   const Layers G = layers_of(g);
@@ -847,11 +910,11 @@ int step_smatrix_layer(rcwa_context* ctx, int N, const double2* erc, const doubl
   const ModeDims d = dims_n(N);
   const size_t NN = (size_t)N * N, nn = (size_t)d.n * d.n;
   const size_t extra = 8 * NN * 16 + 2 * NN * 16 * 2 + 2 * (size_t)N * 4 + 1024 + 16 * 256;
-  int rc = ctx_reserve(ctx, plan_bytes(d, 1) + extra);
+  int rc = ctx_reserve(ctx, plan_bytes(d, 1, 1) + extra);
   if (rc) return rc;
   Plan pl;
-  if ((rc = plan_take(ctx, d, 1, pl))) return rc;
-  Arena a{(char*)ctx->ws + ((plan_bytes(d, 1) + 255) & ~(size_t)255)};
+  if ((rc = plan_take(ctx, d, 1, 1, pl))) return rc;
+  Arena a{(char*)ctx->ws + ((plan_bytes(d, 1, 1) + 255) & ~(size_t)255)};
   rcwa_geometry g;
   g.ctx = ctx;
   g.d = d;
@@ -878,7 +941,9 @@ int step_smatrix_layer(rcwa_context* ctx, int N, const double2* erc, const doubl
   if ((rc = h2d(ctx, pl.wv.Kx, Kx, (size_t)N * 16)) || (rc = h2d(ctx, pl.wv.Ky, Ky, (size_t)N * 16)) ||
       (rc = h2d(ctx, pl.wv.V0, V0d, (size_t)4 * N * 16)) || (rc = h2d(ctx, pl.wv.kinc, kinc, sizeof(kinc))))
     return rc;
-  if ((rc = patterned_layer(ctx, layers_of(&g), 0, pl, dst))) return rc;
+  const Layers G = layers_of(&g);
+  if ((rc = eig_layers(ctx, G, std::vector<int>{0}, pl, dst))) return rc;
+  if ((rc = patterned_layer(ctx, G, 0, pl, pl.Wst, pl.L2st, dst))) return rc;
   if ((rc = d2h(ctx, S11, pl.augD + nn, nn * 16)) || (rc = d2h(ctx, S12, pl.augD + 2 * nn, nn * 16)))
     return rc;
   uint32_t hs[2] = {0, 0};

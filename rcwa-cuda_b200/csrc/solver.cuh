@@ -85,8 +85,9 @@ void geometry_free(rcwa_geometry* g);
 int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* sources, int B,
                  int precision, double* R, double* T, double* tot, uint32_t* status);
 
-// Bytes of device workspace per source for a sweep at this size.
-size_t sweep_bytes_per_source(const ModeDims& d);
+// Bytes of device workspace per source for a sweep at this size with np
+// patterned layers.
+size_t sweep_bytes_per_source(const ModeDims& d, int np);
 
 // Dense building blocks on device pointers (used by the step-level ABI).
 struct SMat {
