@@ -18,6 +18,10 @@ Cases:
                       hole) and one uniform film, lossy eps (Im < 0 in the
                       reference convention), rectangular period 420 x 380 nm,
                       h = (3, 2), a 96 x 80 grid, three oblique sources.
+  golden_c4_m23       the C4 precision-stress stack (20-step staircased
+                      trapezoidal posts on a film over a lossy substrate,
+                      rcwa_b200.configs.c4_trapezoid) at M = 23 (n = 1058),
+                      512 x 512 grids, one wavelength (600 nm), TM.
 """
 from __future__ import annotations
 
@@ -34,7 +38,7 @@ for p in (ROOT, os.path.join(ROOT, "rcwa-cuda_b200"), os.path.dirname(HERE)):
 
 from rcwa_b200 import configs as C  # noqa: E402
 
-CASES = ("golden_small_c1", "golden_small_mixed")
+CASES = ("golden_small_c1", "golden_small_mixed", "golden_c4_m23")
 
 
 def build_case(name: str) -> C.Problem:
@@ -58,6 +62,8 @@ def build_case(name: str) -> C.Problem:
                 C.SourceSpec(745.0, np.radians(5.0), 0.0, 0.7071067811865476, 0.7071067811865476)]
         return C.Problem(name, st, srcs,
                          C.ParamSpec(3, 2, 1.0, 1.0, C.ref_eps(complex(2.25, 0.01)), 1.0))
+    if name == "golden_c4_m23":
+        return C.c4_trapezoid(M=23, lambdas=[600.0])
     raise KeyError(name)
 
 

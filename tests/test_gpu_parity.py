@@ -275,7 +275,7 @@ def test_zero_thickness_and_single_uniform(ctx):
     assert np.abs(a[0] - b[0]).max() < 1e-11 and np.abs(a[1] - b[1]).max() < 1e-11
 
 
-@pytest.mark.parametrize("name", ["golden_small_c1", "golden_small_mixed"])
+@pytest.mark.parametrize("name", ["golden_small_c1", "golden_small_mixed", "golden_c4_m23"])
 def test_golden_fixtures(ctx, name):
     """The CUDA path reproduces the committed fixtures (generated by the
     oracle, tests/golden/make_golden.py) to 1e-10 per order."""
