@@ -49,6 +49,13 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n-lambda", type=int, default=201)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+                    help="c2: the headline sweep (default); c3: batch of uneven requests; "
+                         "c4: large-n precision-stress sweep; c5: Poisson-served requests")
+    ap.add_argument("--count", type=int, default=0, help="c3/c5: number of requests (0 = workload default)")
+    ap.add_argument("--m", type=int, default=31, help="c4: harmonic order M (n = 2 M^2)")
+    ap.add_argument("--rates", default="100,200,500,1000,2000,5000", help="c5: arrival rates (1/s)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     return ap.parse_args()
 
 
@@ -144,6 +151,100 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------- other workloads
+def run_batch_workloads(args):
+    """c3 / c4 / c5 (one GPU, rank 0).  One JSON line each; device work is
+    timed with CUDA events on the library's stream, serving latencies on the
+    host clock from submit to completion."""
+    import torch
+    from rcwa_b200 import lib as L, configs as C
+    prec = L.PREC_MIXED if args.precision == "mixed" else L.PREC_FP64
+    ctx = L.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    line = {"n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128", "data": "synthetic", "precision": args.precision}
+    if args.workload == "c3":
+        count = args.count or 4096
+        pbs = C.c3_batch(count=count)
+        ctx.solve_batch(pbs[:32], precision=prec)          # warm-up (plans, pools)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        ev0.record(stream)
+        R, T, Rt, Tt, st = ctx.solve_batch(pbs, precision=prec)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        ms = ev0.elapsed_time(ev1)
+        line.update({"metric": "C3 uneven batch: solves/s through rcwa_solve_batch (host buffers)",
+                     "value": count / (ms / 1e3), "unit": "solves/s", "steps": 1, "warmup": 1,
+                     "ms_per_step": ms, "wall_s": wall,
+                     "config": {"workload": f"C3: {count} requests, numpy default_rng(3); odd M in 5..21, "
+                                            "1-6 pillar/hole/line layers, 256^2 grids",
+                                "status_nonzero": int((st != 0).sum())}})
+    elif args.workload == "c4":
+        pb = C.c4_trapezoid(M=args.m)
+        st_, par, srcs = pb.stack, pb.params, pb.sources
+        g = ctx.geometry_create(st_, par)
+        B = len(srcs)
+        N = (2 * par.nx_harmonics + 1) * (2 * par.ny_harmonics + 1)
+        R_d = torch.empty(B * N, dtype=torch.float64, device="cuda")
+        T_d = torch.empty(B * N, dtype=torch.float64, device="cuda")
+        tot_d = torch.empty(2 * B, dtype=torch.float64, device="cuda")
+        st_d = torch.empty(B, dtype=torch.int32, device="cuda")
+        ctx.solve_sweep_device(g, srcs[:4], prec, R_d.data_ptr(), T_d.data_ptr(), tot_d.data_ptr(),
+                               st_d.data_ptr())
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        ctx.solve_sweep_device(g, srcs, prec, R_d.data_ptr(), T_d.data_ptr(), tot_d.data_ptr(),
+                               st_d.data_ptr())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        ctx.geometry_destroy(g)
+        tot = tot_d.cpu().numpy().reshape(B, 2)
+        line.update({"metric": "C4 large-n sweep: solves/s (geometry resident, conv matrices built once)",
+                     "value": B / (ms / 1e3), "unit": "solves/s", "steps": 1, "warmup": 1,
+                     "ms_per_step": ms,
+                     "config": {"workload": f"C4: 20-step trapezoid staircase + film, M={args.m} "
+                                            f"(n={2 * args.m * args.m}), 512^2 grids, {B} wavelengths 250-800 nm, TM",
+                                "status_nonzero": int((st_d.cpu().numpy() != 0).sum()),
+                                "R_tot_range": [float(tot[:, 0].min()), float(tot[:, 0].max())]}})
+    else:   # c5
+        count = args.count or 512
+        rng = np.random.default_rng(5)
+        pbs = [C.c3_request(rng, 256, 25) for _ in range(count)]
+        rates = [float(r) for r in args.rates.split(",") if r]
+        res = []
+        for rate in rates:
+            srv = L.Server(0, max_batch=1024, max_queue=1 << 20, precision=prec)
+            try:
+                arr = C.poisson_arrivals(rate, count, seed=int(rate))
+                t0 = time.perf_counter()
+                tickets = []
+                for pb, ta in zip(pbs, arr):
+                    dt = ta - (time.perf_counter() - t0)
+                    if dt > 0:
+                        time.sleep(dt)
+                    tickets.append(srv.submit(pb))
+                for tk, pb in zip(tickets, pbs):
+                    srv.poll(tk, pb, wait=True)
+                span = time.perf_counter() - t0
+                n, p50, p99 = srv.stats()
+            finally:
+                srv.close()
+            res.append({"rate_hz": rate, "served_per_s": count / span, "p50_ms": p50, "p99_ms": p99,
+                        "offered_s": float(arr[-1]), "span_s": span})
+        best = max(r["served_per_s"] for r in res)
+        line.update({"metric": "C5 served requests/s (continuous batching) with p50/p99 latency",
+                     "value": best, "unit": "requests/s", "steps": 1, "warmup": 0,
+                     "config": {"workload": f"C5: {count} C3-distributed requests (M <= 25, n <= 1250) "
+                                            "per rate, Poisson arrivals", "rates": res}})
+    print(json.dumps(line), flush=True)
+
+
 # --------------------------------------------------------------------------- ours
 def main():
     args = parse()
@@ -153,6 +254,10 @@ def main():
     if args.impl == "reference":
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         run_reference(args, rank)
+        return
+    if args.workload != "c2":
+        if rank == 0:
+            run_batch_workloads(args)
         return
 
     import torch

@@ -10,8 +10,12 @@
 // sweep_chunk runs over the whole group with per-item matrices (Layers with
 // s_item != 0), per-item thicknesses and per-item lattice periods.
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
 #include <cstring>
 #include <map>
+#include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -29,18 +33,42 @@ bool grid_uniform(const rcwa_complex* g, size_t G) {
   return true;
 }
 
+// Stacks without uniform layers group regardless of depth (flex = 1, nl = -1):
+// they are sorted deepest first and layer l runs for the leading solves that
+// have it.  Stacks with uniform layers group by exact depth and uniform mask.
 struct GroupKey {
-  int nxh, nyh, nl, nx, ny;
+  int flex, nxh, nyh, nl, nx, ny;
   double p[8];                  // er_ref, ur_ref, er_trn, ur_trn (re, im)
   std::vector<char> uniform;
   bool operator<(const GroupKey& o) const {
-    return std::tie(nxh, nyh, nl, nx, ny, p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], uniform) <
-           std::tie(o.nxh, o.nyh, o.nl, o.nx, o.ny, o.p[0], o.p[1], o.p[2], o.p[3], o.p[4], o.p[5],
+    return std::tie(flex, nxh, nyh, nl, nx, ny, p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], uniform) <
+           std::tie(o.flex, o.nxh, o.nyh, o.nl, o.nx, o.ny, o.p[0], o.p[1], o.p[2], o.p[3], o.p[4], o.p[5],
                     o.p[6], o.p[7], o.uniform);
   }
 };
 
 size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Concurrent group chunks per batch: RCWA_BATCH_STREAMS (read once), default 4.
+int batch_streams() {
+  static int k = -1;
+  if (k < 0) {
+    const char* e = getenv("RCWA_BATCH_STREAMS");
+    k = e ? std::max(1, std::min(16, atoi(e))) : 4;
+  }
+  return k;
+}
+
+// Worker contexts of ctx (created on first use, destroyed with ctx).
+int ensure_workers(rcwa_context* ctx, int K) {
+  while ((int)ctx->workers.size() < K) {
+    rcwa_context* w = nullptr;
+    int rc = rcwa_context_create(ctx->device, &w);
+    if (rc) return rc;
+    ctx->workers.push_back(w);
+  }
+  return RCWA_OK;
+}
 
 // device bytes per item of a group chunk besides the sweep plan
 size_t geometry_bytes_per_item(const ModeDims& d, int nl, int nx, int ny) {
@@ -55,12 +83,26 @@ size_t geometry_bytes_per_item(const ModeDims& d, int nl, int nx, int ny) {
   return b + 1024;
 }
 
-// One group chunk: items idx[0..B) share key k.
-int run_chunk(rcwa_context* ctx, const GroupKey& k, const std::vector<int>& idx,
+// One group chunk: items idx0[0..B) share key k0.
+int run_chunk(rcwa_context* ctx, const GroupKey& k0, const std::vector<int>& idx0,
               const rcwa_stack* stacks, const rcwa_source* sources, const rcwa_params* params,
               rcwa_result* out, bool& any_status) {
   cudaStream_t s = ctx->stream;
-  const int B = (int)idx.size();
+  const int B = (int)idx0.size();
+  // the chunk's budget comes from its own context (workers get a share)
+  // deepest stacks first; layer l belongs to the first nb[l] items
+  std::vector<int> idx(idx0);
+  GroupKey k = k0;
+  std::vector<int> nb;
+  if (k.flex) {
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](int a, int b) { return stacks[a].num_layers > stacks[b].num_layers; });
+    k.nl = stacks[idx[0]].num_layers;
+    k.uniform.assign(k.nl, 0);
+    nb.assign(k.nl, 0);
+    for (int i : idx)
+      for (int l = 0; l < stacks[i].num_layers; ++l) ++nb[l];
+  }
   const rcwa_params& p0 = params[idx[0]];
   ModeDims d;
   d.nxh = p0.nx_harmonics;
@@ -111,20 +153,23 @@ int run_chunk(rcwa_context* ctx, const GroupKey& k, const std::vector<int>& idx,
     return rc;
 
   // grids: er of every item's layers, then ur, in [item][layer][ny][nx] order
+  // (slots past a shorter stack's depth stay zero and are never read)
+  if (k.flex && L > 0) RCWA_CUDA_TRY(cudaMemsetAsync(grids, 0, 2 * L * G * sizeof(double2), s));
   for (int b = 0; b < B; ++b) {
     const rcwa_stack& st = stacks[idx[b]];
-    if (nl == 0) break;
-    RCWA_CUDA_TRY(cudaMemcpyAsync(grids + (size_t)b * nl * G, st.er, nl * G * sizeof(double2),
+    const int lb = st.num_layers;
+    if (lb == 0) continue;
+    RCWA_CUDA_TRY(cudaMemcpyAsync(grids + (size_t)b * nl * G, st.er, lb * G * sizeof(double2),
                                   cudaMemcpyHostToDevice, s));
-    RCWA_CUDA_TRY(cudaMemcpyAsync(grids + L * G + (size_t)b * nl * G, st.ur, nl * G * sizeof(double2),
+    RCWA_CUDA_TRY(cudaMemcpyAsync(grids + L * G + (size_t)b * nl * G, st.ur, lb * G * sizeof(double2),
                                   cudaMemcpyHostToDevice, s));
   }
   // per-item layer scalars
-  std::vector<double> ht(L);
-  std::vector<double2> he(L), hm(L);
+  std::vector<double> ht(L, 0.0);
+  std::vector<double2> he(L, make_double2(1, 0)), hm(L, make_double2(1, 0));
   for (int b = 0; b < B; ++b) {
     const rcwa_stack& st = stacks[idx[b]];
-    for (int l = 0; l < nl; ++l) {
+    for (int l = 0; l < st.num_layers; ++l) {
       ht[(size_t)b * nl + l] = st.t[l];
       const rcwa_complex e = st.er[(size_t)l * G], m = st.ur[(size_t)l * G];
       he[(size_t)b * nl + l] = make_double2(e.re, e.im);
@@ -140,38 +185,33 @@ int run_chunk(rcwa_context* ctx, const GroupKey& k, const std::vector<int>& idx,
     if ((rc = convmat(s, grids + L * G, (int)L, k.nx, k.ny, d, urc, scr))) return rc;
   }
   // inverses of the patterned layers: one LU batch over (item, layer, field)
-  std::vector<int> pat;
-  for (int l = 0; l < nl; ++l)
-    if (!k.uniform[l]) pat.push_back(l);
-  const int np = (int)pat.size();
-  if (np > 0) {
-    const size_t nsys = (size_t)2 * B * np;
+  std::vector<size_t> slots;   // b * nl + l of every patterned layer present
+  for (int b = 0; b < B; ++b)
+    for (int l = 0; l < stacks[idx[b]].num_layers; ++l)
+      if (!k.uniform[l]) slots.push_back((size_t)b * nl + l);
+  const size_t ns = slots.size();
+  if (ns > 0) {
+    const size_t nsys = 2 * ns;
     const long long s2 = 2 * (long long)NN;
     if ((rc = dalloc(nsys * s2 * sizeof(double2), (void**)&aug)) ||
         (rc = dalloc(nsys * d.N * sizeof(int), (void**)&piv)) ||
         (rc = dalloc(nsys * sizeof(uint32_t), (void**)&gst)))
       return rc;
-    for (int b = 0; b < B; ++b)
-      for (int q = 0; q < np; ++q) {
-        const size_t src = ((size_t)b * nl + pat[q]) * NN;
-        const size_t sys = (size_t)b * np + q;
-        RCWA_CUDA_TRY(cudaMemcpyAsync(aug + sys * s2, erc + src, NN * sizeof(double2),
-                                      cudaMemcpyDeviceToDevice, s));
-        RCWA_CUDA_TRY(cudaMemcpyAsync(aug + ((size_t)B * np + sys) * s2, urc + src, NN * sizeof(double2),
-                                      cudaMemcpyDeviceToDevice, s));
-      }
+    for (size_t q = 0; q < ns; ++q) {
+      RCWA_CUDA_TRY(cudaMemcpyAsync(aug + q * s2, erc + slots[q] * NN, NN * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, s));
+      RCWA_CUDA_TRY(cudaMemcpyAsync(aug + (ns + q) * s2, urc + slots[q] * NN, NN * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, s));
+    }
     if ((rc = set_identity(s, aug, d.N, d.N, s2, 2 * d.N, d.N, (int)nsys, make_double2(1, 0)))) return rc;
     RCWA_CUDA_TRY(cudaMemsetAsync(gst, 0, nsys * sizeof(uint32_t), s));
     if ((rc = zgesv(s, d.N, d.N, aug, d.N, s2, (int)nsys, piv, gst))) return rc;
-    for (int b = 0; b < B; ++b)
-      for (int q = 0; q < np; ++q) {
-        const size_t dstl = ((size_t)b * nl + pat[q]) * NN;
-        const size_t sys = (size_t)b * np + q;
-        RCWA_CUDA_TRY(cudaMemcpyAsync(einv + dstl, aug + sys * s2 + NN, NN * sizeof(double2),
-                                      cudaMemcpyDeviceToDevice, s));
-        RCWA_CUDA_TRY(cudaMemcpyAsync(uinv + dstl, aug + ((size_t)B * np + sys) * s2 + NN,
-                                      NN * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-      }
+    for (size_t q = 0; q < ns; ++q) {
+      RCWA_CUDA_TRY(cudaMemcpyAsync(einv + slots[q] * NN, aug + q * s2 + NN, NN * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, s));
+      RCWA_CUDA_TRY(cudaMemcpyAsync(uinv + slots[q] * NN, aug + (ns + q) * s2 + NN, NN * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, s));
+    }
   }
 
   Layers Gl;
@@ -191,6 +231,7 @@ int run_chunk(rcwa_context* ctx, const GroupKey& k, const std::vector<int>& idx,
   Gl.t_item = t_d;
   Gl.ueps_item = ueps_d;
   Gl.umu_item = umu_d;
+  Gl.nb = k.flex ? nb.data() : nullptr;
 
   std::vector<SourceDev> hs(B);
   for (int b = 0; b < B; ++b) {
@@ -231,6 +272,7 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
     set_last_error("unknown precision mode %d", precision);
     return RCWA_ERR_INVALID;
   }
+  cudaGetLastError();   // no stale error from earlier unchecked calls on this thread
   // group by shape, keeping the order of first appearance
   std::map<GroupKey, int> gid;
   std::vector<GroupKey> keys;
@@ -249,8 +291,16 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
     std::memcpy(k.p, pv, sizeof(pv));
     const size_t G = (size_t)st.nx * st.ny;
     k.uniform.resize(st.num_layers);
-    for (int l = 0; l < st.num_layers; ++l)
+    bool any_uniform = false;
+    for (int l = 0; l < st.num_layers; ++l) {
       k.uniform[l] = (grid_uniform(st.er + l * G, G) && grid_uniform(st.ur + l * G, G)) ? 1 : 0;
+      any_uniform = any_uniform || k.uniform[l];
+    }
+    k.flex = (st.num_layers > 0 && !any_uniform) ? 1 : 0;
+    if (k.flex) {
+      k.nl = -1;
+      k.uniform.clear();
+    }
     auto it = gid.find(k);
     if (it == gid.end()) {
       it = gid.emplace(k, (int)keys.size()).first;
@@ -280,7 +330,15 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
     ~TcScope() { c->tc = 0; }
   } tc_scope{ctx};
   ctx->tc = precision == RCWA_PREC_MIXED ? 1 : 0;
-  bool any_status = false;
+  // chunks of every group, sized for a share of the budget each, so that
+  // several can run at once
+  const int kmax = batch_streams();
+  struct Job {
+    int g;
+    std::vector<int> idx;
+    double cost;
+  };
+  std::vector<Job> jobs;
   for (size_t g = 0; g < keys.size(); ++g) {
     const GroupKey& k = keys[g];
     ModeDims d;
@@ -290,18 +348,99 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
     d.Q = 2 * d.nyh + 1;
     d.N = d.P * d.Q;
     d.n = 2 * d.N;
-    int np = 0;
-    for (int l = 0; l < k.nl; ++l) np += k.uniform[l] ? 0 : 1;
-    const size_t per = sweep_bytes_per_source(d, np) + geometry_bytes_per_item(d, k.nl, k.nx, k.ny);
-    int chunk = (int)std::max<size_t>(1, budget / per);
-    if (max_group > 0) chunk = std::min(chunk, max_group);
     const std::vector<int>& m = members[g];
+    int nl = k.nl, np = 0;
+    if (k.flex) {
+      nl = 0;
+      for (int i : m) nl = std::max(nl, stacks[i].num_layers);
+      np = nl;
+    } else {
+      for (int l = 0; l < k.nl; ++l) np += k.uniform[l] ? 0 : 1;
+    }
+    const size_t per = sweep_bytes_per_source(d, np) + geometry_bytes_per_item(d, nl, k.nx, k.ny);
+    int chunk = (int)std::max<size_t>(1, budget / kmax / per);
+    // launch grids index matrices in a 65535-wide grid dimension: at most
+    // 2 * layers * items systems per batched LU
+    chunk = std::min(chunk, std::max(1, 32000 / std::max(1, 2 * std::max(nl, 1))));
+    if (max_group > 0) chunk = std::min(chunk, max_group);
     for (size_t b0 = 0; b0 < m.size(); b0 += chunk) {
       const size_t bc = std::min<size_t>(chunk, m.size() - b0);
-      std::vector<int> idx(m.begin() + b0, m.begin() + b0 + bc);
-      int rc = run_chunk(ctx, k, idx, stacks, sources, params, out, any_status);
+      Job j{(int)g, std::vector<int>(m.begin() + b0, m.begin() + b0 + bc), 0.0};
+      for (int i : j.idx) j.cost += (double)d.n * d.n * d.n * (stacks[i].num_layers + 2);
+      jobs.push_back(std::move(j));
+    }
+  }
+  const int K = std::min<int>(kmax, (int)jobs.size());
+  std::atomic<bool> any_status{false};
+  if (K <= 1) {
+    for (const Job& j : jobs) {
+      bool st = false;
+      int rc = run_chunk(ctx, keys[j.g], j.idx, stacks, sources, params, out, st);
+      if (st) any_status = true;
       if (rc) return rc;
     }
+  } else {
+    // independent groups run concurrently, one worker context (own stream
+    // and workspace) and host thread each; longest jobs are placed first
+    std::vector<int> order(jobs.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return jobs[a].cost > jobs[b].cost; });
+    std::vector<std::vector<int>> bins(K);
+    std::vector<double> load(K, 0.0);
+    for (int j : order) {
+      const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      bins[w].push_back(j);
+      load[w] += jobs[j].cost;
+    }
+    int rc = ensure_workers(ctx, K);
+    if (rc) return rc;
+    // the workers' streams follow the caller's stream and the caller's
+    // stream waits for them, so events on it bracket the whole batch
+    cudaEvent_t start;
+    RCWA_CUDA_TRY(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+    RCWA_CUDA_TRY(cudaEventRecord(start, ctx->stream));
+    std::vector<int> rcs(K, RCWA_OK);
+    std::vector<std::string> errs(K);
+    std::vector<std::thread> th;
+    for (int w = 0; w < K; ++w) {
+      th.emplace_back([&, w] {
+        rcwa_context* wc = ctx->workers[w];
+        wc->tc = ctx->tc;
+        cudaError_t e = cudaSetDevice(wc->device);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(wc->stream, start, 0);
+        cudaGetLastError();   // launch checks below must see only their own launches
+        if (e != cudaSuccess) {
+          rcs[w] = RCWA_ERR_CUDA;
+          errs[w] = std::string("batch worker set-up: ") + cudaGetErrorString(e);
+          return;
+        }
+        for (int j : bins[w]) {
+          bool st = false;
+          int r = run_chunk(wc, keys[jobs[j].g], jobs[j].idx, stacks, sources, params, out, st);
+          if (st) any_status = true;
+          if (r) {
+            rcs[w] = r;
+            errs[w] = rcwa_last_error();
+            break;
+          }
+        }
+        wc->tc = 0;
+      });
+    }
+    for (auto& t : th) t.join();
+    for (int w = 0; w < K; ++w) {
+      cudaEvent_t done;
+      RCWA_CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+      RCWA_CUDA_TRY(cudaEventRecord(done, ctx->workers[w]->stream));
+      RCWA_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, done, 0));
+      RCWA_CUDA_TRY(cudaEventDestroy(done));
+    }
+    RCWA_CUDA_TRY(cudaEventDestroy(start));
+    for (int w = 0; w < K; ++w)
+      if (rcs[w]) {
+        set_last_error("%s", errs[w].c_str());
+        return rcs[w];
+      }
   }
   if (tc_err) {
     int h = 0;
@@ -312,7 +451,7 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
       return RCWA_ERR_CUDA;
     }
   }
-  return any_status ? RCWA_ERR_NUMERIC : RCWA_OK;
+  return any_status.load() ? RCWA_ERR_NUMERIC : RCWA_OK;
 }
 
 }  // namespace rcwa

@@ -110,6 +110,8 @@ int rcwa_context_create(int device, rcwa_context** out) {
 int rcwa_context_destroy(rcwa_context* c) {
   if (!c) return RCWA_OK;
   cudaSetDevice(c->device);
+  for (rcwa_context* w : c->workers) rcwa_context_destroy(w);
+  c->workers.clear();
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->ws) cudaFree(c->ws);
   if (c->pinned) cudaFreeHost(c->pinned);

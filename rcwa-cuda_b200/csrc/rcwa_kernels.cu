@@ -637,10 +637,13 @@ int convmat(cudaStream_t s, const double2* grids, int nl, int nx, int ny, const 
   RCWA_LAUNCH_CHECK();
   const size_t shm = (size_t)2 * nx * sizeof(double2);
   if (shm > 48 * 1024) {
-    static bool set = false;
-    if (!set) {
-      cudaFuncSetAttribute(convmat_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-      set = true;
+    static bool set[64] = {};   // the attribute is per device
+    int dev = 0;
+    RCWA_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64 || !set[dev]) {
+      RCWA_CUDA_TRY(cudaFuncSetAttribute(convmat_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024));
+      if (dev < 64) set[dev] = true;
     }
     if (shm > 200 * 1024) {
       set_last_error("convmat: nx=%d too large", nx);

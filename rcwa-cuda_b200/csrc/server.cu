@@ -14,6 +14,7 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -35,6 +36,7 @@ struct Request {
   double R_tot = 0, T_tot = 0;
   uint32_t status = 0;
   int rc = 0;
+  std::string err;   // the solver's message when rc is an error
   bool done = false;
   Clock::time_point t_submit, t_done;
 };
@@ -92,6 +94,7 @@ void serve(rcwa_server* S) {
     }
     const int rc = rcwa::solve_batch(S->ctx, n, st.data(), src.data(), par.data(), S->precision,
                                      S->max_batch, out.data());
+    const std::string msg = (rc == RCWA_OK || rc == RCWA_ERR_NUMERIC) ? std::string() : rcwa_last_error();
     const auto now = Clock::now();
     {
       std::lock_guard<std::mutex> lk(S->mu);
@@ -102,8 +105,10 @@ void serve(rcwa_server* S) {
         r->status = out[i].status;
         if (rc == RCWA_OK || rc == RCWA_ERR_NUMERIC)
           r->rc = out[i].status ? RCWA_ERR_NUMERIC : RCWA_OK;
-        else
+        else {
           r->rc = rc;
+          r->err = msg;
+        }
         r->done = true;
         r->t_done = now;
         S->lat_ms.push_back(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
@@ -220,6 +225,7 @@ int rcwa_server_poll(rcwa_server* S, uint64_t ticket, int wait, rcwa_result* out
     out->status = r->status;
   }
   const int rc = r->rc;
+  if (rc && rc != RCWA_ERR_NUMERIC) rcwa::set_last_error("%s", r->err.c_str());
   S->reqs.erase(it);
   return rc;
 }

@@ -403,26 +403,42 @@ int layer_omega2(rcwa_context* ctx, const Layers& g, int l, Plan& pl, double2* o
 }
 
 // Eigen-decompositions (rcwa.cpp:298-306) of the patterned layers `pat` of the
-// chunk, all in ONE batched eigensolver call of np * B matrices (more
-// independent matrices per launch fill the SMs better than one launch per
-// layer).  Layer pat[k] of source b: W at pl.Wst + (k B + b) n^2, lambda^2 at
-// pl.L2st + (k B + b) n.
+// chunk, all in ONE batched eigensolver call (more independent matrices per
+// launch fill the SMs better than one launch per layer).  Layer pat[k] holds
+// the first nb(pat[k]) sources of the chunk; its matrices are packed after
+// those of pat[0..k): W at pl.Wst + (off_k + b) n^2, lambda^2 at
+// pl.L2st + (off_k + b) n, off_k = sum of the earlier layers' counts.
 int eig_layers(rcwa_context* ctx, const Layers& g, const std::vector<int>& pat, Plan& pl,
                uint32_t* status) {
   cudaStream_t s = ctx->stream;
-  const int B = pl.B, n = g.d.n, np = (int)pat.size();
-  if (np == 0) return RCWA_OK;
-  if (np > pl.np) {
-    set_last_error("internal: plan sized for %d patterned layers, %d needed", pl.np, np);
+  const int n = g.d.n, np = (int)pat.size();
+  long long total = 0;
+  for (int k = 0; k < np; ++k) total += g.items(pat[k], pl.B);
+  if (total == 0) return RCWA_OK;
+  if (total > (long long)pl.np * pl.B) {
+    set_last_error("internal: plan sized for %d x %d layer eigenproblems, %lld needed", pl.np, pl.B, total);
     return RCWA_ERR_INVALID;
   }
   const long long nn = (long long)n * n;
   int rc;
-  for (int k = 0; k < np; ++k)
-    if ((rc = layer_omega2(ctx, g, pat[k], pl, pl.OmA + (size_t)k * B * nn))) return rc;
-  RCWA_CUDA_TRY(cudaMemsetAsync(pl.est, 0, (size_t)np * B * sizeof(uint32_t), s));
-  if ((rc = zeig(s, n, np * B, pl.OmA, n, nn, pl.Wst, nn, pl.L2st, n, pl.est, pl.eigws))) return rc;
-  return fold_status(s, status, pl.est, B, np);
+  long long off = 0;
+  for (int k = 0; k < np; ++k) {
+    Plan plk = pl;
+    plk.B = g.items(pat[k], pl.B);
+    if (plk.B == 0) continue;
+    if ((rc = layer_omega2(ctx, g, pat[k], plk, pl.OmA + off * nn))) return rc;
+    off += plk.B;
+  }
+  RCWA_CUDA_TRY(cudaMemsetAsync(pl.est, 0, (size_t)total * sizeof(uint32_t), s));
+  if ((rc = zeig(s, n, (int)total, pl.OmA, n, nn, pl.Wst, nn, pl.L2st, n, pl.est, pl.eigws))) return rc;
+  off = 0;
+  for (int k = 0; k < np; ++k) {
+    const int Bl = g.items(pat[k], pl.B);
+    if (Bl == 0) continue;
+    if ((rc = fold_status(s, status, pl.est + off, Bl, 1))) return rc;
+    off += Bl;
+  }
+  return RCWA_OK;
 }
 
 // S-matrix of one patterned layer (rcwa.cpp:254-352) for the chunk, from its
@@ -696,48 +712,71 @@ int sweep_chunk_layers(rcwa_context* ctx, const Layers& g, const SourceDev* hsrc
   }
   double2* tmp = pl.tmp;
   const long long sL = 8LL * d.N;     // BD uniform layer: S11 (4N) + S12 (4N) per source
-  std::vector<int> pat, slot(g.nl, -1);
-  for (int l = 0; l < g.nl; ++l)
-    if (!g.uniform[l]) {
-      slot[l] = (int)pat.size();
-      pat.push_back(l);
-    }
+  std::vector<int> pat;
+  std::vector<long long> off(g.nl, 0);
+  {
+    long long o = 0;
+    for (int l = 0; l < g.nl; ++l)
+      if (!g.uniform[l]) {
+        off[l] = o;
+        o += g.items(l, B);
+        pat.push_back(l);
+      }
+  }
   if ((rc = eig_layers(ctx, g, pat, pl, status))) return rc;
+  // sources without layer 0 (only in batches of stacks of different depth)
+  // start from the empty-stack S-matrix (rcwa.cpp:237-250)
+  if (g.nl > 0 && g.items(0, B) < B) {
+    const int b0 = g.items(0, B), c = B - b0;
+    for (int k = 0; k < 4; ++k)
+      if ((rc = fill_zero(s, dev.p[k] + (size_t)b0 * nn, (size_t)c * nn))) return rc;
+    if ((rc = set_identity(s, dev.p[1] + (size_t)b0 * nn, n, n, nn, n, 0, c, make_double2(1, 0)))) return rc;
+    if ((rc = set_identity(s, dev.p[2] + (size_t)b0 * nn, n, n, nn, n, 0, c, make_double2(1, 0)))) return rc;
+  }
   for (int l = 0; l < g.nl; ++l) {
+    const int Bl = g.items(l, B);   // this layer belongs to sources 0 .. Bl-1
+    if (Bl == 0) continue;
+    double2* const S12_before = dev.p[1];
     if (g.uniform[l]) {
-      if ((rc = uniform_layer(s, B, d, g.ueps ? g.ueps[l] : make_double2(1, 0),
+      if ((rc = uniform_layer(s, Bl, d, g.ueps ? g.ueps[l] : make_double2(1, 0),
                               g.umu ? g.umu[l] : make_double2(1, 0), g.t ? g.t[l] : 0.0,
                               g.ueps_item ? g.ueps_item + l : nullptr, g.umu_item ? g.umu_item + l : nullptr,
                               g.t_item ? g.t_item + l : nullptr, g.nl, pl.wv, pl.lbd, pl.lbd + 4 * d.N, sL, 1)))
         return rc;
       if (l == 0) {
         // S_init (x) S_layer == S_layer exactly (S11 = S22 = 0, S12 = S21 = I)
-        if ((rc = bd_dense(s, d.N, pl.lbd, sL, dev.p[0], nn, 0, B))) return rc;
-        if ((rc = bd_dense(s, d.N, pl.lbd + 4 * d.N, sL, dev.p[1], nn, 0, B))) return rc;
-        if ((rc = bd_dense(s, d.N, pl.lbd + 4 * d.N, sL, dev.p[2], nn, 0, B))) return rc;
-        if ((rc = bd_dense(s, d.N, pl.lbd, sL, dev.p[3], nn, 0, B))) return rc;
+        if ((rc = bd_dense(s, d.N, pl.lbd, sL, dev.p[0], nn, 0, Bl))) return rc;
+        if ((rc = bd_dense(s, d.N, pl.lbd + 4 * d.N, sL, dev.p[1], nn, 0, Bl))) return rc;
+        if ((rc = bd_dense(s, d.N, pl.lbd + 4 * d.N, sL, dev.p[2], nn, 0, Bl))) return rc;
+        if ((rc = bd_dense(s, d.N, pl.lbd, sL, dev.p[3], nn, 0, Bl))) return rc;
       } else {
-        RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
-        if ((rc = star_product_bd(ctx, B, d, dev, pl.lbd, sL, tmp, pl.augFG, pl.piv, pl.st))) return rc;
-        if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
+        RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * (size_t)Bl * sizeof(uint32_t), s));
+        if ((rc = star_product_bd(ctx, Bl, d, dev, pl.lbd, sL, tmp, pl.augFG, pl.piv, pl.st))) return rc;
+        if ((rc = fold_status(s, status, pl.st, Bl, 2))) return rc;
       }
-      continue;
-    }
-    const size_t k = (size_t)slot[l];
-    if ((rc = patterned_layer(ctx, g, l, pl, pl.Wst + k * B * nn, pl.L2st + k * B * n, status))) return rc;
-    SMat lay;
-    lay.p[0] = pl.augD + nn; lay.s[0] = s3;      // S11 = D^-1 R1
-    lay.p[1] = pl.augD + 2 * nn; lay.s[1] = s3;  // S12 = D^-1 X R2
-    lay.p[2] = lay.p[1]; lay.s[2] = lay.s[1];    // S21 = S12 (:351)
-    lay.p[3] = lay.p[0]; lay.s[3] = lay.s[0];    // S22 = S11
-    if (l == 0) {
-      for (int k = 0; k < 4; ++k)
-        if ((rc = copy_blocks(s, dev.p[k], dev.s[k], lay.p[k], lay.s[k], nn, B))) return rc;
     } else {
-      RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
-      if ((rc = star_product(ctx, B, n, dev, lay, tmp, pl.augFG, pl.piv, pl.st))) return rc;
-      if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
+      Plan plk = pl;
+      plk.B = Bl;
+      if ((rc = patterned_layer(ctx, g, l, plk, pl.Wst + off[l] * nn, pl.L2st + off[l] * n, status))) return rc;
+      SMat lay;
+      lay.p[0] = pl.augD + nn; lay.s[0] = s3;      // S11 = D^-1 R1
+      lay.p[1] = pl.augD + 2 * nn; lay.s[1] = s3;  // S12 = D^-1 X R2
+      lay.p[2] = lay.p[1]; lay.s[2] = lay.s[1];    // S21 = S12 (:351)
+      lay.p[3] = lay.p[0]; lay.s[3] = lay.s[0];    // S22 = S11
+      if (l == 0) {
+        for (int k = 0; k < 4; ++k)
+          if ((rc = copy_blocks(s, dev.p[k], dev.s[k], lay.p[k], lay.s[k], nn, Bl))) return rc;
+      } else {
+        RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * (size_t)Bl * sizeof(uint32_t), s));
+        if ((rc = star_product(ctx, Bl, n, dev, lay, tmp, pl.augFG, pl.piv, pl.st))) return rc;
+        if ((rc = fold_status(s, status, pl.st, Bl, 2))) return rc;
+      }
     }
+    // the star products leave the new S12 in the former scratch block: carry
+    // the S12 of the sources past Bl (which skip this layer) across
+    if (Bl < B && dev.p[1] != S12_before)
+      if ((rc = copy_blocks(s, dev.p[1] + (size_t)Bl * nn, nn, S12_before + (size_t)Bl * nn, nn, nn, B - Bl)))
+        return rc;
   }
   if (g.nl == 0) {
     for (int k = 0; k < 4; ++k) {

@@ -24,6 +24,9 @@ struct rcwa_context {
   // assembly, star products, their LU solves) uses split-TF32 tensor-core
   // GEMMs; Omega^2 and the eigensolver stay FP64
   int tc = 0;
+  // worker contexts (own stream + workspace) that run independent group
+  // chunks of rcwa_solve_batch concurrently; owned by this context
+  std::vector<rcwa_context*> workers;
 };
 
 struct rcwa_geometry {
@@ -64,6 +67,11 @@ struct Layers {
   const double* t_item = nullptr;
   const double2* ueps_item = nullptr;
   const double2* umu_item = nullptr;
+  // host [nl] (may be null): layer l belongs to the first nb[l] solves of the
+  // chunk only (a batch of stacks of different depth, sorted deepest first);
+  // the other solves pass through that layer unchanged
+  const int* nb = nullptr;
+  int items(int l, int B) const { return nb ? (nb[l] < B ? nb[l] : B) : B; }
 };
 Layers layers_of(const rcwa_geometry* g);
 // One chunk of B solves (device outputs R/T [B][N], tot [B][2], status [B]);
