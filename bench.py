@@ -123,30 +123,36 @@ class ClockSampler:
 
 # --------------------------------------------------------------------------- reference arm
 def run_reference(args, rank):
+    """The reference's CPU path (the FP64 port in oracle/) on all host cores:
+    one single-threaded solve per process, one process per core; a step is
+    one wavelength per process."""
     if rank != 0:
         return
-    from helpers_bench import oracle_one_solve
+    from helpers_bench import OraclePool
     pb = workload(args.n_lambda)
-    # bounded sample: one wavelength per step, cycling through non-anomalous points
+    # cycle through the non-anomalous wavelengths (400 and 600 nm are Rayleigh points)
     idx = [i for i in range(len(pb.sources)) if i not in (0, 100)]
-    convs = None
-    times = []
-    for s in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        convs = oracle_one_solve(pb, idx[(s * 37) % len(idx)], convs)
-        dt = time.perf_counter() - t0
-        if s >= args.warmup:
-            times.append(dt)
+    pool = OraclePool(pb)
+    P = pool.procs
+    try:
+        times = []
+        for s in range(args.warmup + args.steps):
+            sel = [idx[(s * P + j) * 37 % len(idx)] for j in range(P)]
+            _, dt = pool.run(sel)
+            if s >= args.warmup:
+                times.append(dt)
+    finally:
+        pool.close()
     tot = sum(times)
-    value = args.steps / tot
-    cores = os.cpu_count()
+    value = args.steps * P / tot
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": WORKLOAD_DESC, "sample": "1 solve per step (conv matrices hoisted after the first)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "1 wavelength of the sweep per step; NumPy/SciPy FP64 restatement, OpenBLAS threads = all host cores"},
+            "config": {"workload": WORKLOAD_DESC,
+                       "sample": f"{P} wavelengths per step, one per process (conv matrices built once per process)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": P, "kind": "port",
+                             "sample": f"{P} single-threaded processes x 1 wavelength per step; NumPy/SciPy FP64 restatement"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -332,13 +338,13 @@ def main():
     # event pairs around every launch of the hot kernels (kept out of `value`)
     L.profile_reset()
     L.profile_enable(True)
-    pa, pb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    pa.record(stream)
+    prof_a, prof_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    prof_a.record(stream)
     step_device()
-    pb.record(stream)
+    prof_b.record(stream)
     barrier()
     L.profile_enable(False)
-    prof_step_ms = pa.elapsed_time(pb)
+    prof_step_ms = prof_a.elapsed_time(prof_b)
     fam = {}
     # disjoint families ("hess" brackets the whole blocked reduction incl. its GEMMs)
     for name in ("zgemm", "zgemm_rank", "hess_panel", "schur", "trevc", "lu_panel"):
@@ -404,6 +410,20 @@ def main():
                                                     if hess_all[0] else None)
     shares["hess(blocked, incl. its GEMMs)"] = round(hess_all[0] / max(1e-9, prof_step_ms), 4)
 
+    # DRAM traffic per launch of the dominant family, from ncu captures of the
+    # same kernels on this workload (profiles/), scaled by the units per launch
+    traffic, traffic_src = None, None
+    if dom == "schur":
+        per_matrix = (17.125991e9 + 19.132079e9) / 48          # schur24 capture: 48 matrices
+        traffic = per_matrix * 2 * B                             # 2 patterned layers x B sources per launch
+        traffic_src = ("ncu dram__bytes_read+write of schur_kernel on 48 n=450 matrices of this workload "
+                       "(profiles/schur_kernel_c2_n450_batch48.md), scaled to the 2 x %d matrices of one launch" % B)
+    elif dom == "zgemm":
+        per_flop = (155.732992e6 + 52.608e6) / (24 * 8 * 450.0 ** 3)   # dmma24 capture
+        traffic = per_flop * (dfl / dn) if dn else None
+        traffic_src = ("ncu dram bytes of zgemm_dmma_kernel on the 24 x 450^3 Omega^2 GEMM "
+                       "(profiles/zgemm_dmma_c2_omega2_n450_batch24.md), scaled by flops per launch")
+
     solves = B * args.steps * world
     value = solves / (dev_ms / 1e3)
     e2e_val = solves / (e2e_ms / 1e3)
@@ -412,22 +432,25 @@ def main():
     cpu = None
     err = None
     if not args.no_cpu_baseline:
+        # one single-threaded oracle process per host core, one wavelength each
         sys.path.insert(0, os.path.join(ROOT, "tests"))
-        from helpers_bench import oracle_one_solve_result
-        t0 = time.perf_counter()
-        ref_res = []
-        sample_idx = [26, 167]   # 452 nm and 734 nm (not anomalous)
-        convs = None
-        for i in sample_idx:
-            res, convs = oracle_one_solve_result(pb, i, convs)
-            ref_res.append(res)
-        cpu_t = time.perf_counter() - t0
-        cpu = {"value": len(sample_idx) / cpu_t, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-               "sample": f"{len(sample_idx)} wavelengths of the sweep (incl. conv matrices once), NumPy/SciPy FP64 restatement, OpenBLAS on all host threads"}
+        from helpers_bench import OraclePool
+        pool = OraclePool(pb)
+        try:
+            P = pool.procs
+            idx = [i for i in range(len(srcs)) if i not in (0, 100)]
+            sample_idx = [idx[(j * 37) % len(idx)] for j in range(P)]
+            res, cpu_t = pool.run(sample_idx)
+        finally:
+            pool.close()
+        cpu = {"value": len(sample_idx) / cpu_t, "unit": UNIT, "cores": P, "kind": "port",
+               "sample": f"{P} wavelengths of the sweep, one per single-threaded process on {P} host cores "
+                         "(NumPy/SciPy FP64 restatement; conv matrices built once per process, outside the timing)"}
         err = 0.0
-        for i, res in zip(sample_idx, ref_res):
+        for i in sample_idx:
+            _, Rr, Tr, Rt, Tt, _ = res[i]
             R_gpu = R_h[i].reshape(2 * par.nx_harmonics + 1, 2 * par.ny_harmonics + 1).T
-            err = max(err, float(np.abs(R_gpu - res.R).max()), abs(float(tot_h[i, 1]) - res.T_tot))
+            err = max(err, float(np.abs(R_gpu - Rr).max()), abs(float(tot_h[i, 1]) - Tt))
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -444,7 +467,7 @@ def main():
         "gpu_launches": int(launches),
         "roofline": {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": zgemm_peak,
                      "unit": "TFLOP/s", "frac": (achieved / zgemm_peak) if achieved else None,
-                     "traffic": None,
+                     "traffic": traffic, "traffic_source": traffic_src,
                      "peak_source": "cuBLAS ZGEMM 4096^3 (complex128) measured in this run",
                      "launches": dn, "avg_launch_ms": dms / dn if dn else None,
                      "family_time_share": shares, "family_tflops": fam_tflops},
