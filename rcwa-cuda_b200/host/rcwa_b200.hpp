@@ -317,4 +317,75 @@ inline Results Solve(const Device& device, const Source& source, const RCWAParam
   return SolveSweep(device, std::vector<Source>{source}, params, precision)[0];
 }
 
+// ---- batches of unrelated problems and the serving loop ------------------------
+struct Problem {
+  const Device* device;
+  Source source;
+  RCWAParams params;
+};
+
+// rcwa_solve_batch: every problem has its own stack, source and port media.
+inline std::vector<Results> SolveBatch(const std::vector<Problem>& problems,
+                                       int precision = RCWA_PREC_FP64) {
+  const int n = (int)problems.size();
+  std::vector<Results> res(n);
+  std::vector<rcwa_stack> st(n);
+  std::vector<rcwa_source> cs(n);
+  std::vector<rcwa_params> cp(n);
+  std::vector<rcwa_result> out(n);
+  for (int i = 0; i < n; ++i) {
+    const Problem& q = problems[i];
+    st[i] = q.device->c_stack();
+    cs[i] = q.source.c_source();
+    cp[i] = q.params.c_params();
+    res[i].R = RealMatrix(q.params.Q(), q.params.P());
+    res[i].T = RealMatrix(q.params.Q(), q.params.P());
+    out[i] = rcwa_result{res[i].R.data(), res[i].T.data(), 0.0, 0.0, 0u};
+  }
+  if (n > 0) check(rcwa_solve_batch(Context(), n, st.data(), cs.data(), cp.data(), precision, out.data()));
+  for (int i = 0; i < n; ++i) {
+    res[i].R_tot = out[i].R_tot;
+    res[i].T_tot = out[i].T_tot;
+    res[i].status = out[i].status;
+  }
+  return res;
+}
+
+// rcwa_server_*: requests are queued from any thread and solved in batches
+// by the server's worker (continuous batching).
+class Server {
+ public:
+  explicit Server(int device = 0, int max_batch = 256, int max_queue = 1 << 20,
+                  int precision = RCWA_PREC_FP64) {
+    check(rcwa_server_create(device, max_batch, max_queue, precision, &h_));
+  }
+  ~Server() { rcwa_server_destroy(h_); }
+  Server(const Server&) = delete;
+  Server& operator=(const Server&) = delete;
+  uint64_t Submit(const Device& device, const Source& source, const RCWAParams& params) {
+    rcwa_stack st = device.c_stack();
+    rcwa_source cs = source.c_source();
+    rcwa_params cp = params.c_params();
+    uint64_t t = 0;
+    check(rcwa_server_submit(h_, &st, &cs, &cp, &t));
+    return t;
+  }
+  // Blocks until the request is done; the ticket is released.
+  Results Wait(uint64_t ticket, const RCWAParams& params) {
+    Results r;
+    r.R = RealMatrix(params.Q(), params.P());
+    r.T = RealMatrix(params.Q(), params.P());
+    rcwa_result out{r.R.data(), r.T.data(), 0.0, 0.0, 0u};
+    int done = 0;
+    check(rcwa_server_poll(h_, ticket, 1, &out, &done));
+    r.R_tot = out.R_tot;
+    r.T_tot = out.T_tot;
+    r.status = out.status;
+    return r;
+  }
+
+ private:
+  rcwa_server* h_ = nullptr;
+};
+
 }  // namespace rcwa_b200
