@@ -139,9 +139,18 @@ int zeig(cudaStream_t s, int n, int batch, double2* A, int ld, long long sA, dou
     set_last_error("zeig: n=%d too large", n);
     return RCWA_ERR_INVALID;
   }
-  if (trevc_shm > 48 * 1024)
-    RCWA_CUDA_TRY(cudaFuncSetAttribute(trevc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)trevc_shm));
+  if (trevc_shm > 48 * 1024) {
+    // per function and device, shared by all threads: set the bound once, not
+    // this call's size (a concurrent call with a smaller n would undercut it)
+    static bool set[64] = {};
+    int dev = 0;
+    RCWA_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64 || !set[dev]) {
+      RCWA_CUDA_TRY(cudaFuncSetAttribute(trevc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024));
+      if (dev < 64) set[dev] = true;
+    }
+  }
   void* tok = nullptr;
   (void)tau;
   {

@@ -212,8 +212,17 @@ int hess_blocked(cudaStream_t s, int n, int batch, double2* A, double2* Z, doubl
       set_last_error("hess: n=%d too large", n);
       return RCWA_ERR_INVALID;
     }
-    RCWA_CUDA_TRY(cudaFuncSetAttribute(hess_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)shm));
+    // the attribute is per function and device, shared by every thread: set
+    // the bound once instead of this call's size (concurrent callers with
+    // different n would otherwise undercut each other's launches)
+    static bool set[64] = {};
+    int dev = 0;
+    RCWA_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64 || !set[dev]) {
+      RCWA_CUDA_TRY(cudaFuncSetAttribute(hess_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024));
+      if (dev < 64) set[dev] = true;
+    }
   }
   auto gemm = [&](int m, int ncol, int kd, double2 alpha, const double2* X, int ldx, long long sx,
                   int opx, const double2* Yb, int ldy, long long sy, int opy, double2 beta,

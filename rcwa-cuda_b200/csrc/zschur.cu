@@ -31,7 +31,7 @@ namespace rcwa {
 namespace {
 using namespace eig;
 
-constexpr int NT = 128;                      // 2 CTAs/SM at <= 255 registers, no spills
+constexpr int NT = 256;                      // 8 warps: the chase warp + 7 update warps, 1 CTA/SM
 constexpr int SW = 16;                      // single-shift reflectors per chunk
 constexpr int SWIN = SW + 3;
 constexpr int NS = 8;                        // bulges per multishift sweep
@@ -479,7 +479,7 @@ __device__ void multi_sweep(Smem& sm, double2* stage, double2* H, double2* Z, in
   }
 }
 
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, 1)
 schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2* __restrict__ Zg,
              double2* __restrict__ lamg, long long slam, uint32_t* __restrict__ status,
              int max_sweeps_per_n) {
