@@ -16,21 +16,37 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // 2x2 Householder reflector (zlarfg with n = 2): beta (real), tau, v2 with
 // (I - tau [1 v2]^T [1 v2]^* )^H [alpha; x] = [beta; 0].
+// It sits on the serial critical path of every QR chase step, so the common
+// case uses one square root and two divisions: the norm is formed unscaled
+// when all components lie in [1e-140, 1e140] (no over- or underflow of the
+// squares), v2 = x conj(d) / |d|^2 with d = alpha - beta (|d| >= |beta|).
+// Other magnitudes take the scaled path.
 __device__ __forceinline__ void larfg2(double2 alpha, double2 x, double& beta, double2& tau,
                                        double2& v2) {
-  const double xn = hypot(x.x, x.y);
-  if (xn == 0.0 && alpha.y == 0.0) {
+  if (x.x == 0.0 && x.y == 0.0 && alpha.y == 0.0) {
     tau = cmk(0.0, 0.0);
     v2 = cmk(0.0, 0.0);
     beta = alpha.x;
     return;
   }
-  const double mx = fmax(fmax(fabs(alpha.x), fabs(alpha.y)), xn);
-  const double a = alpha.x / mx, c = alpha.y / mx, d = xn / mx;
-  const double nrm = mx * sqrt(a * a + c * c + d * d);
+  const double mx = fmax(fmax(fabs(alpha.x), fabs(alpha.y)), fmax(fabs(x.x), fabs(x.y)));
+  double nrm;
+  if (mx > 1e-140 && mx < 1e140) {
+    nrm = sqrt(fma(alpha.x, alpha.x, fma(alpha.y, alpha.y, fma(x.x, x.x, x.y * x.y))));
+  } else {
+    const double a = alpha.x / mx, c = alpha.y / mx, e = x.x / mx, f = x.y / mx;
+    nrm = mx * sqrt(a * a + c * c + e * e + f * f);
+  }
   beta = -copysign(nrm, alpha.x);
-  tau = cmk((beta - alpha.x) / beta, -alpha.y / beta);
-  v2 = cmul(x, crcp(cmk(alpha.x - beta, alpha.y)));
+  const double rb = 1.0 / beta;
+  tau = cmk((beta - alpha.x) * rb, -alpha.y * rb);
+  const double2 d = cmk(alpha.x - beta, alpha.y);
+  if (mx > 1e-140 && mx < 1e140) {
+    const double rd = 1.0 / fma(d.x, d.x, d.y * d.y);
+    v2 = cmk((x.x * d.x + x.y * d.y) * rd, (x.y * d.x - x.x * d.y) * rd);
+  } else {
+    v2 = cmul(x, crcp(d));
+  }
 }
 
 // Left application of G^H = I - conj(tau) v v^H, v = [1, v2], to (a; q).

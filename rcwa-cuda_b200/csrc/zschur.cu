@@ -479,6 +479,275 @@ __device__ void multi_sweep(Smem& sm, double2* stage, double2* H, double2* Z, in
   }
 }
 
+// ---- aggressive early deflation (zlaqr3 rules) ---------------------------------
+// The trailing NWIN x NWIN window of the active block [l, i] is brought to
+// Schur form T = V^H H_w V by one warp (single-shift QR with full T and V).
+// With s = H(kw, kw-1) the coupling entry, the window's coupling column
+// becomes the spike s conj(V(0, :)); eigenvalue j of T is deflatable when
+// |s| |V(0, j)| <= max(smlnum, ulp |T(j, j)|) (tested upward from the
+// bottom, stopping at the first failure).  If nd > 0 of them deflate, the
+// spike of the k = NWIN - nd others is folded into its first entry by one
+// reflector, T(0:k, 0:k) is reduced back to Hessenberg form, and V is applied
+// to the rest of H (rows above, columns to the right) and to Z.  The k
+// undeflated eigenvalues serve as the next sweep's shifts.
+constexpr int NWIN = 16;                     // AED window
+constexpr int LDW = NWIN + 1;                // column stride of the window arrays
+constexpr int AED_MIN = NWIN + 16;           // smallest active block that gets AED
+
+struct AedBuf {      // carved from the dynamic staging area (not used meanwhile)
+  double2* T;        // [NWIN][LDW] window, T[col * LDW + row]
+  double2* V;        // [NWIN][LDW] Schur vectors
+  double2* v;        // [32] current reflector
+  double2* sp;       // [32] spike
+};
+__device__ __forceinline__ AedBuf aed_buf(double2* stage) {
+  AedBuf a;
+  a.T = stage;
+  a.V = stage + NWIN * LDW;
+  a.v = stage + 2 * NWIN * LDW;
+  a.sp = a.v + 32;
+  return a;
+}
+
+// Warp-level reflector for x[0..len) held as x = lane < len ? xi : 0:
+// H^H x = beta e1 with H = I - tau v v^H, v[0] = 1 (zlarfg).  Writes v to vs.
+__device__ __forceinline__ void warp_larfg(double2 xi, int len, int lane, double2* vs, double2& tau,
+                                           double& beta) {
+  double2 a0;   // alpha = x[0]
+  a0.x = __shfl_sync(0xffffffffu, xi.x, 0);
+  a0.y = __shfl_sync(0xffffffffu, xi.y, 0);
+  const double xn2 = warp_sum((lane >= 1 && lane < len) ? xi.x * xi.x + xi.y * xi.y : 0.0);
+  if (xn2 == 0.0 && a0.y == 0.0) {
+    tau = cmk(0.0, 0.0);
+    beta = a0.x;
+    if (lane < len) vs[lane] = lane == 0 ? cmk(1.0, 0.0) : cmk(0.0, 0.0);
+    __syncwarp();
+    return;
+  }
+  // scaled norm against overflow (values here are O(|H|))
+  const double nrm = sqrt(a0.x * a0.x + a0.y * a0.y + xn2);
+  beta = -copysign(nrm, a0.x);
+  tau = cmk((beta - a0.x) / beta, -a0.y / beta);
+  const double2 sc = crcp(cmk(a0.x - beta, a0.y));
+  if (lane < len) vs[lane] = lane == 0 ? cmk(1.0, 0.0) : cmul(xi, sc);
+  __syncwarp();
+}
+
+// Left application of H^H to rows [r0, r0+len) of window columns [c0, NWIN)
+// (one lane per column).
+__device__ __forceinline__ void warp_left(double2* T, const double2* v, double2 tau, int r0, int len,
+                                          int c0, int lane) {
+  const int c = lane;
+  if (c >= c0 && c < NWIN) {
+    double2* col = T + c * LDW + r0;
+    double2 w = cmk(0.0, 0.0);
+    for (int j = 0; j < len; ++j) w = cadd(w, cmulc(v[j], col[j]));
+    const double2 sw = cmulc(tau, w);
+    for (int j = 0; j < len; ++j) col[j] = csub(col[j], cmul(v[j], sw));
+  }
+  __syncwarp();
+}
+// Right application of H to columns [c0, c0+len) of rows [0, rmax) of A
+// (one lane per row).
+__device__ __forceinline__ void warp_right(double2* A, const double2* v, double2 tau, int c0, int len,
+                                           int rmax, int lane) {
+  const int r = lane;
+  if (r < rmax) {
+    double2 w = cmk(0.0, 0.0);
+    for (int j = 0; j < len; ++j) w = cadd(w, cmul(A[(c0 + j) * LDW + r], v[j]));
+    const double2 sw = cmul(tau, w);
+    for (int j = 0; j < len; ++j) {
+      double2& a = A[(c0 + j) * LDW + r];
+      a = csub(a, cmulc(v[j], sw));
+    }
+  }
+  __syncwarp();
+}
+
+// Schur form of the NWIN x NWIN Hessenberg window (full T, V accumulated),
+// one warp.  False when the iteration cap is reached or a shift is not finite.
+__device__ bool win_schur(double2* T, double2* V, int lane) {
+  const double ulp = DBL_EPSILON;
+  int ii = NWIN - 1, its = 0, total = 0;
+  auto t = [&](int r, int c) -> double2& { return T[c * LDW + r]; };
+  while (ii > 0) {
+    bool neg = false;
+    if (lane >= 1 && lane <= ii) {
+      const double ah = cabs1(t(lane, lane - 1));
+      neg = ah <= ulp * (cabs1(t(lane - 1, lane - 1)) + cabs1(t(lane, lane))) || ah < DBL_MIN;
+    }
+    const unsigned msk = __ballot_sync(0xffffffffu, neg);
+    const int ll = msk ? 31 - __clz(msk) : 0;
+    if (ll == ii) {
+      if (lane == 0) t(ii, ii - 1) = cmk(0.0, 0.0);
+      __syncwarp();
+      --ii;
+      its = 0;
+      continue;
+    }
+    if (ll > 0 && lane == 0) t(ll, ll - 1) = cmk(0.0, 0.0);
+    if (++total > 30 * NWIN * 4) return false;
+    ++its;
+    double2 mu;
+    if (its % 10 == 0)
+      mu = cadd(t(ii, ii), cmk(0.75 * fabs(t(ii, ii - 1).x), 0.0));
+    else
+      mu = wilkinson_shift(t(ii - 1, ii - 1), t(ii - 1, ii), t(ii, ii - 1), t(ii, ii));
+    if (!cfinite(mu)) return false;
+    __syncwarp();
+    for (int k = ll; k < ii; ++k) {
+      double2 alpha, x;
+      if (k == ll) {
+        alpha = csub(t(k, k), mu);
+        x = t(k + 1, k);
+      } else {
+        alpha = t(k, k - 1);
+        x = t(k + 1, k - 1);
+      }
+      double beta;
+      double2 tau, v2;
+      larfg2(alpha, x, beta, tau, v2);
+      __syncwarp();
+      if (k > ll && lane == 0) {
+        t(k, k - 1) = cmk(beta, 0.0);
+        t(k + 1, k - 1) = cmk(0.0, 0.0);
+      }
+      if (lane >= k && lane < NWIN) refl_left(T[lane * LDW + k], T[lane * LDW + k + 1], tau, v2);
+      __syncwarp();
+      if (lane <= min(k + 2, ii)) refl_right(T[k * LDW + lane], T[(k + 1) * LDW + lane], tau, v2);
+      if (lane < NWIN) refl_right(V[k * LDW + lane], V[(k + 1) * LDW + lane], tau, v2);
+      __syncwarp();
+    }
+  }
+  return true;
+}
+
+// Y[0:len) <- Y V (row vector times the window's V), Y strided by ys.
+__device__ __forceinline__ void row_times_v(double2* Y, long long ys, const double2* V) {
+  double2 y[NWIN];
+#pragma unroll
+  for (int j = 0; j < NWIN; ++j) y[j] = Y[j * ys];
+#pragma unroll 1
+  for (int q = 0; q < NWIN; ++q) {
+    double2 acc = cmk(0.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < NWIN; ++j) cfma(acc, y[j], V[q * LDW + j]);
+    Y[q * ys] = acc;
+  }
+}
+// Y[0:len) <- V^H Y (column vector), Y strided by ys.
+__device__ __forceinline__ void vh_times_col(double2* Y, long long ys, const double2* V) {
+  double2 y[NWIN];
+#pragma unroll
+  for (int j = 0; j < NWIN; ++j) y[j] = Y[j * ys];
+#pragma unroll 1
+  for (int q = 0; q < NWIN; ++q) {
+    double2 acc = cmk(0.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < NWIN; ++j) acc = cadd(acc, cmulc(V[q * LDW + j], y[j]));
+    Y[q * ys] = acc;
+  }
+}
+
+// V applied outside the window: H rows [0, kw), H columns (i, n), Z rows.
+__device__ __noinline__ void aed_apply(const double2* V, double2* H, double2* Z, int ld, int n, int kw,
+                                       int i) {
+  const int nA = kw, nB = n - 1 - i, total = nA + nB + n;
+  for (int it = threadIdx.x; it < total; it += NT) {
+    if (it < nA)
+      row_times_v(H + (long long)kw * ld + it, ld, V);
+    else if (it < nA + nB)
+      vh_times_col(H + (long long)(i + 1 + it - nA) * ld + kw, 1, V);
+    else
+      row_times_v(Z + (long long)kw * ld + (it - nA - nB), ld, V);
+  }
+}
+
+// AED on the active block [l, i] (i - l + 1 >= AED_MIN).  Returns the number
+// of deflated eigenvalues (-1 when the window QR failed: H unchanged).  When
+// at least NS eigenvalues stay undeflated, the bottom NS of them are written
+// to sm.shifts and sm.flag is set to 2.
+__device__ int aed(Smem& sm, double2* stage, double2* H, double2* Z, int ld, int n, int l, int i,
+                   double smlnum) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const double ulp = DBL_EPSILON;
+  const AedBuf A = aed_buf(stage);
+  const int kw = i - NWIN + 1;
+  for (int e = tid; e < NWIN * NWIN; e += NT) {
+    const int r = e % NWIN, c = e / NWIN;
+    A.T[c * LDW + r] = (r <= c + 1) ? H[(long long)(kw + c) * ld + kw + r] : cmk(0.0, 0.0);
+    A.V[c * LDW + r] = cmk(r == c ? 1.0 : 0.0, 0.0);
+  }
+  __syncthreads();
+  if (wid == 0) {
+    if (lane == 0) sm.flag = 0;
+    __syncwarp();
+    const bool ok = win_schur(A.T, A.V, lane);
+    int nd = -1;
+    if (ok) {
+      const double2 sp = (kw > l) ? H[(long long)(kw - 1) * ld + kw] : cmk(0.0, 0.0);
+      // deflation test upward from the bottom
+      bool defl = false;
+      if (lane < NWIN) {
+        double foo = cabs1(A.T[lane * LDW + lane]);
+        if (foo == 0.0) foo = cabs1(sp);
+        defl = cabs1(sp) * cabs1(A.V[lane * LDW + 0]) <= fmax(smlnum, ulp * foo);
+      }
+      const unsigned dm = __ballot_sync(0xffffffffu, defl) & ((1u << NWIN) - 1);
+      // trailing run of deflatable eigenvalues: lanes NWIN-1 downward
+      const unsigned inv = (~dm) & ((1u << NWIN) - 1);
+      nd = inv ? (NWIN - 1 - (31 - __clz(inv))) : NWIN;
+      const int k = NWIN - nd;
+      if (lane < NS && k >= NS) sm.shifts[lane] = A.T[(k - NS + lane) * LDW + (k - NS + lane)];
+      if (lane == 0) sm.flag = (k >= NS) ? 2 : 0;
+      if (nd > 0) {
+        // spike of the undeflated part, s conj(V(0, j)), j < k
+        const double2 spj = (lane < k) ? cmul(sp, cconj(A.V[lane * LDW + 0])) : cmk(0.0, 0.0);
+        if (k > 1 && (sp.x != 0.0 || sp.y != 0.0)) {
+          double2 tau;
+          double beta;
+          warp_larfg(spj, k, lane, A.v, tau, beta);
+          warp_left(A.T, A.v, tau, 0, k, 0, lane);
+          warp_right(A.T, A.v, tau, 0, k, k, lane);
+          warp_right(A.V, A.v, tau, 0, k, NWIN, lane);
+          if (lane < NWIN) A.sp[lane] = lane == 0 ? cmk(beta, 0.0) : cmk(0.0, 0.0);
+          __syncwarp();
+          // back to Hessenberg form: T(0:k, 0:k)
+          for (int c = 0; c + 2 < k; ++c) {
+            const int len = k - c - 1;
+            const double2 xi = (lane < len) ? A.T[c * LDW + c + 1 + lane] : cmk(0.0, 0.0);
+            double2 tg;
+            double bg;
+            warp_larfg(xi, len, lane, A.v, tg, bg);
+            warp_left(A.T, A.v, tg, c + 1, len, c + 1, lane);
+            if (lane < len) A.T[c * LDW + c + 1 + lane] = lane == 0 ? cmk(bg, 0.0) : cmk(0.0, 0.0);
+            __syncwarp();
+            warp_right(A.T, A.v, tg, c + 1, len, k, lane);
+            warp_right(A.V, A.v, tg, c + 1, len, NWIN, lane);
+          }
+        } else {
+          if (lane < NWIN) A.sp[lane] = (lane < k) ? spj : cmk(0.0, 0.0);
+          __syncwarp();
+        }
+      }
+    }
+    if (lane == 0) sm.l = nd;   // broadcast (sm.l is rewritten by the next scan)
+  }
+  __syncthreads();
+  const int nd = sm.l;
+  if (nd <= 0) return nd;
+  // write back the window (zero below the subdiagonal) and the spike column
+  for (int e = tid; e < NWIN * NWIN; e += NT) {
+    const int r = e % NWIN, c = e / NWIN;
+    H[(long long)(kw + c) * ld + kw + r] = (r <= c + 1) ? A.T[c * LDW + r] : cmk(0.0, 0.0);
+  }
+  if (kw > l)
+    for (int r = tid; r < NWIN; r += NT) H[(long long)(kw - 1) * ld + kw + r] = A.sp[r];
+  aed_apply(A.V, H, Z, ld, n, kw, i);
+  __syncthreads();
+  return nd;
+}
+
 __global__ void __launch_bounds__(NT, 1)
 schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2* __restrict__ Zg,
              double2* __restrict__ lamg, long long slam, uint32_t* __restrict__ status,
@@ -541,10 +810,29 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
       if (++total > sweep_cap) break;
       const int m = i - l + 1;
       if (m >= MS_MIN) {
-        // NS shifts: eigenvalues of the trailing NS x NS block, or exceptional
+        // aggressive early deflation first (large blocks)
+        int ib = i;             // bottom of the block the sweep chases
+        bool aed_shifts = false;
+        if (m >= AED_MIN) {
+          const long long c4 = clock64();
+          const int nd = aed(sm, stage, H, Z, ld, n, l, i, smlnum);
+          SCHUR_STAT(13, 1);
+          SCHUR_STAT(15, clock64() - c4);
+          if (nd > 0) {
+            SCHUR_STAT(14, nd);
+            kdefl = 0;
+            // many deflations, or too little left: rescan before sweeping
+            if (nd * 100 > NWIN * 14 || (i - nd) - l + 1 < MS_MIN) continue;
+            ib = i - nd;
+          }
+          aed_shifts = nd >= 0 && sm.flag == 2;
+          __syncthreads();
+        }
+        // NS shifts: the window's undeflated eigenvalues, else the eigenvalues
+        // of the trailing NS x NS block, or exceptional ones
         bool exc = (kdefl % 6 == 0);
-        if (!exc) {
-          const int q0 = i - NS + 1;
+        if (!exc && !aed_shifts) {
+          const int q0 = ib - NS + 1;
           for (int e = tid; e < NS * NS; e += NT) {
             const int r = e % NS, c = e / NS;
             sm.Hs[c][r] = (r <= c + 1) ? H[(long long)(q0 + c) * ld + q0 + r] : cmk(0.0, 0.0);
@@ -565,13 +853,13 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
         if (exc) {
           SCHUR_STAT(5, 1);
           if (tid < NS) {   // zlaqr0: H(k,k) + 0.75 |H(k,k-1)| down the trailing diagonal
-            const int k = i - tid;
+            const int k = ib - tid;
             sm.shifts[tid] = cadd(H[(long long)k * ld + k], cmk(0.75 * cabs1(H[(long long)(k - 1) * ld + k]), 0.0));
           }
           __syncthreads();
         }
         const long long c1 = clock64();
-        multi_sweep(sm, stage, H, Z, ld, n, l, i);
+        multi_sweep(sm, stage, H, Z, ld, n, l, ib);
         SCHUR_STAT(0, 1);
         SCHUR_STAT(2, clock64() - c1);
       } else {
