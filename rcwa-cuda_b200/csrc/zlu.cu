@@ -6,18 +6,23 @@
 // block M = [A | B] (n rows, n + nrhs columns); on return the A part holds U
 // (and the L multipliers) and the B part holds the solution.
 //
-// Blocked right-looking elimination with panel width NB:
-//   panel   : one CTA per matrix factors the n-j x NB panel (pivot search,
-//             row swaps inside the panel, scaling, rank-1 updates);
-//   swap+L  : one thread per trailing column applies the panel's row swaps and
-//             the unit-lower NB x NB forward substitution (U12 = L11^-1 A12);
-//   update  : the trailing block [A22 | B2] -= L21 * [U12 | Y1] runs as a
-//             batched GEMM (zgemm), which carries almost all the flops.
-// Back substitution with U runs block-wise: NB x NB upper solve per block,
-// then a GEMM update of the rows above.
-//
-// Row swaps are applied to the trailing columns only: L is consumed on the fly
-// by the right-hand sides, so the columns left of the panel are never needed.
+// 1. P A = L U by blocked right-looking elimination over the A columns, with
+//    panel width NB:
+//      panel  : one CTA per matrix factors the n-j x NB panel (pivot search,
+//               row swaps inside the panel, scaling, rank-1 updates);
+//      swap+L : one thread per trailing column applies the panel's row swaps
+//               and the unit-lower NB x NB forward substitution;
+//      update : the trailing block A22 -= L21 U12 as a batched GEMM.
+//    Each panel's interchanges are applied to the columns on both sides, so
+//    the stored multipliers form L of P A = L U (LAPACK's convention).
+// 2. the right-hand sides get all row swaps at once (B <- P B);
+// 3. L Y = P B and U X = Y by recursive halving: each off-diagonal block is
+//    one GEMM with k up to n/2, only NB x NB diagonal blocks are solved by the
+//    column kernels.  With many right-hand sides (the [A | I] and [D | R | R']
+//    systems of the S-matrix algebra) this moves most of the flops from
+//    rank-NB updates onto large-k GEMMs.
+#include <functional>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -116,7 +121,7 @@ lu_panel_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int j
 // columns [c_begin, c_end) of the augmented matrix.
 __global__ void __launch_bounds__(COL_NT)
 lu_swap_lsolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int j, int jb,
-                      int c_begin, int c_end, const int* __restrict__ pivg) {
+                      int c_begin, int c_end, const int* __restrict__ pivg, int swap) {
   const int b = blockIdx.y;
   double2* M = Mg + (long long)b * stride;
   const int* piv = pivg + (long long)b * n;
@@ -127,19 +132,21 @@ lu_swap_lsolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int n,
     int r = e % jb, c = e / jb;
     L[r][c] = M[(long long)(j + c) * ld + j + r];
   }
-  for (int e = tid; e < jb; e += COL_NT) sp[e] = piv[j + e];
+  if (swap)
+    for (int e = tid; e < jb; e += COL_NT) sp[e] = piv[j + e];
   __syncthreads();
   const int col = c_begin + blockIdx.x * COL_NT + tid;
   if (col >= c_end) return;
   double2* q = M + (long long)col * ld;
-  for (int c = 0; c < jb; ++c) {
-    int p = sp[c];
-    if (p != j + c) {
-      double2 t = q[j + c];
-      q[j + c] = q[p];
-      q[p] = t;
+  if (swap)
+    for (int c = 0; c < jb; ++c) {
+      int p = sp[c];
+      if (p != j + c) {
+        double2 t = q[j + c];
+        q[j + c] = q[p];
+        q[p] = t;
+      }
     }
-  }
   double2 x[NB];
 #pragma unroll
   for (int c = 0; c < NB; ++c) x[c] = (c < jb) ? q[j + c] : cmk(0.0, 0.0);
@@ -157,6 +164,28 @@ lu_swap_lsolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int n,
 #pragma unroll
   for (int c = 0; c < NB; ++c)
     if (c < jb) q[j + c] = x[c];
+}
+
+// Row interchanges piv[r_begin..r_end) (in order) applied to columns
+// [c_begin, c_end): the multipliers left of a panel, and the right-hand sides
+// (B <- P B).
+__global__ void __launch_bounds__(COL_NT)
+lu_rowswap_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int r_begin, int r_end,
+                  int c_begin, int c_end, const int* __restrict__ pivg) {
+  const int b = blockIdx.y;
+  double2* M = Mg + (long long)b * stride;
+  const int* piv = pivg + (long long)b * n;
+  const int col = c_begin + blockIdx.x * COL_NT + threadIdx.x;
+  if (col >= c_end) return;
+  double2* q = M + (long long)col * ld;
+  for (int r = r_begin; r < r_end; ++r) {
+    const int p = piv[r];
+    if (p != r) {
+      const double2 t = q[r];
+      q[r] = q[p];
+      q[p] = t;
+    }
+  }
 }
 
 // Upper-triangular solve X = U11^-1 X for rows j..j+jb-1 of the right-hand
@@ -205,6 +234,27 @@ int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride,
           int* piv, uint32_t* status, int tc) {
   if (n <= 0 || batch <= 0) return RCWA_OK;
   const int ncols = n + nrhs;
+  auto gemm = [&](int m, int nc, int k, const double2* A, const double2* Bm, double2* C) {
+    ZGemm gm;
+    gm.m = m;
+    gm.n = nc;
+    gm.k = k;
+    gm.alpha = cmk(-1.0, 0.0);
+    gm.beta = cmk(1.0, 0.0);
+    gm.A = A;
+    gm.lda = ld;
+    gm.sA = stride;
+    gm.B = Bm;
+    gm.ldb = ld;
+    gm.sB = stride;
+    gm.C = C;
+    gm.ldc = ld;
+    gm.sC = stride;
+    gm.batch = batch;
+    gm.tc = tc;
+    return zgemm(s, gm);
+  };
+  // 1. P A = L U, right-looking over the A columns only
   for (int j = 0; j < n; j += NB) {
     const int jb = (n - j < NB) ? (n - j) : NB;
     void* tok = prof_begin(s);
@@ -212,67 +262,69 @@ int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride,
     prof_end(s, tok, "lu_panel");
     count_launch();
     RCWA_LAUNCH_CHECK();
-    const int cb = j + jb;
-    if (cb < ncols) {
-      dim3 g(cdiv_up(ncols - cb, COL_NT), batch);
-      lu_swap_lsolve_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, jb, cb, ncols, piv);
+    if (j > 0) {   // the earlier multipliers follow this panel's interchanges (P A = L U)
+      dim3 g(cdiv_up(j, COL_NT), batch);
+      lu_rowswap_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, j + jb, 0, j, piv);
       count_launch();
       RCWA_LAUNCH_CHECK();
-      if (cb < n) {
-        ZGemm gm;
-        gm.m = n - cb;
-        gm.n = ncols - cb;
-        gm.k = jb;
-        gm.alpha = cmk(-1.0, 0.0);
-        gm.beta = cmk(1.0, 0.0);
-        gm.A = M + (long long)j * ld + cb;
-        gm.lda = ld;
-        gm.sA = stride;
-        gm.B = M + (long long)cb * ld + j;
-        gm.ldb = ld;
-        gm.sB = stride;
-        gm.C = M + (long long)cb * ld + cb;
-        gm.ldc = ld;
-        gm.sC = stride;
-        gm.batch = batch;
-        gm.tc = tc;
-        int rc = zgemm(s, gm);
-        if (rc) return rc;
-      }
     }
-  }
-  if (nrhs <= 0) return RCWA_OK;
-  const int nblk = (n + NB - 1) / NB;
-  for (int bi = nblk - 1; bi >= 0; --bi) {
-    const int j = bi * NB;
-    const int jb = (n - j < NB) ? (n - j) : NB;
-    dim3 g(cdiv_up(nrhs, COL_NT), batch);
-    lu_usolve_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, j, jb, n, ncols);
-    count_launch();
-    RCWA_LAUNCH_CHECK();
-    if (j > 0) {
-      ZGemm gm;
-      gm.m = j;
-      gm.n = nrhs;
-      gm.k = jb;
-      gm.alpha = cmk(-1.0, 0.0);
-      gm.beta = cmk(1.0, 0.0);
-      gm.A = M + (long long)j * ld;
-      gm.lda = ld;
-      gm.sA = stride;
-      gm.B = M + (long long)n * ld + j;
-      gm.ldb = ld;
-      gm.sB = stride;
-      gm.C = M + (long long)n * ld;
-      gm.ldc = ld;
-      gm.sC = stride;
-      gm.batch = batch;
-      gm.tc = tc;
-      int rc = zgemm(s, gm);
+    const int cb = j + jb;
+    if (cb < n) {
+      dim3 g(cdiv_up(n - cb, COL_NT), batch);
+      lu_swap_lsolve_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, jb, cb, n, piv, 1);
+      count_launch();
+      RCWA_LAUNCH_CHECK();
+      int rc = gemm(n - cb, n - cb, jb, M + (long long)j * ld + cb, M + (long long)cb * ld + j,
+                    M + (long long)cb * ld + cb);
       if (rc) return rc;
     }
   }
-  return RCWA_OK;
+  if (nrhs <= 0) return RCWA_OK;
+  // 2. B <- P B
+  double2* Bc = M + (long long)n * ld;   // right-hand sides, rows 0..n-1
+  {
+    dim3 g(cdiv_up(nrhs, COL_NT), batch);
+    lu_rowswap_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, n, 0, n, n, ncols, piv);
+    count_launch();
+    RCWA_LAUNCH_CHECK();
+  }
+  // 3./4. L Y = P B, then U X = Y, by recursive halving: the off-diagonal
+  // blocks become GEMMs with k up to n/2 (tensor-core sized), only the
+  // diagonal NB x NB blocks are solved by the column kernels
+  auto split = [](int r0, int r1) { return r0 + NB * (((r1 - r0 + NB - 1) / NB) / 2); };
+  int rc = RCWA_OK;
+  std::function<int(int, int)> lower = [&](int r0, int r1) -> int {
+    if (r1 - r0 <= NB) {
+      dim3 g(cdiv_up(nrhs, COL_NT), batch);
+      lu_swap_lsolve_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, n, r0, r1 - r0, n, ncols, piv, 0);
+      count_launch();
+      RCWA_LAUNCH_CHECK();
+      return RCWA_OK;
+    }
+    const int mid = split(r0, r1);
+    int r = lower(r0, mid);
+    if (r) return r;
+    r = gemm(r1 - mid, nrhs, mid - r0, M + (long long)r0 * ld + mid, Bc + r0, Bc + mid);
+    if (r) return r;
+    return lower(mid, r1);
+  };
+  std::function<int(int, int)> upper = [&](int r0, int r1) -> int {
+    if (r1 - r0 <= NB) {
+      dim3 g(cdiv_up(nrhs, COL_NT), batch);
+      lu_usolve_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, r0, r1 - r0, n, ncols);
+      count_launch();
+      RCWA_LAUNCH_CHECK();
+      return RCWA_OK;
+    }
+    const int mid = split(r0, r1);
+    int r = upper(mid, r1);
+    if (r) return r;
+    r = gemm(mid - r0, nrhs, r1 - mid, M + (long long)mid * ld + r0, Bc + mid, Bc + r0);
+    if (r) return r;
+    return upper(r0, mid);
+  };
+  if ((rc = lower(0, n))) return rc;
+  return upper(0, n);
 }
 
 }  // namespace rcwa
