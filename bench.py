@@ -414,7 +414,7 @@ def main():
     # same kernels on this workload (profiles/), scaled by the units per launch
     traffic, traffic_src = None, None
     if dom == "schur":
-        per_matrix = (17.125991e9 + 19.132079e9) / 48          # schur24 capture: 48 matrices
+        per_matrix = (11.669982e9 + 13.266891e9) / 48          # schur24 capture: 48 matrices
         traffic = per_matrix * 2 * B                             # 2 patterned layers x B sources per launch
         traffic_src = ("ncu dram__bytes_read+write of schur_kernel on 48 n=450 matrices of this workload "
                        "(profiles/schur_kernel_c2_n450_batch48.md), scaled to the 2 x %d matrices of one launch" % B)

@@ -114,6 +114,29 @@ def test_eig_batched_and_structured(ctx):
     assert np.abs(A[1] @ W[1] - W[1] * lam[1][None, :]).max() < 1e-9 * np.abs(A[1]).max() * n
 
 
+def test_eig_aed_paths(ctx):
+    """Matrices large enough for aggressive early deflation (active blocks of
+    32 or more): a random one, one with clusters of nearly equal eigenvalues
+    (many window eigenvalues deflate at once), an exactly degenerate
+    diagonalisable one, and an upper-triangular-plus-noise one whose
+    eigenvalues are mostly converged on entry."""
+    rng = np.random.default_rng(17)
+    n = 160
+    Q = np.linalg.qr(_rand(rng, n, n))[0]
+    clus = np.repeat(_rand(rng, n // 8), 8) + 1e-9 * _rand(rng, n)
+    degen = np.repeat(_rand(rng, n // 4), 4)
+    T = np.diag(10.0 * _rand(rng, n)) + 0.1 * np.triu(_rand(rng, n, n), 1) + 1e-13 * _rand(rng, n, n)
+    mats = [_rand(rng, n, n), Q @ np.diag(clus) @ Q.conj().T, Q @ np.diag(degen) @ Q.conj().T, T]
+    A = np.stack(mats)
+    lam, W, st = ctx.eig(A)
+    assert not st.any()
+    for i in (0, 1, 3):
+        _eig_check(A[i], lam[i], W[i])
+    ref = np.sort_complex(degen)
+    assert np.abs(np.sort_complex(lam[2]) - ref).max() < 1e-9 * np.abs(ref).max()
+    assert np.abs(A[2] @ W[2] - W[2] * lam[2][None, :]).max() < 1e-9 * np.abs(A[2]).max() * n
+
+
 def test_eig_nonfinite_flagged(ctx):
     A = np.eye(6, dtype=complex)
     A[2, 3] = np.nan
