@@ -15,12 +15,15 @@
 //      update : the trailing block A22 -= L21 U12 as a batched GEMM.
 //    Each panel's interchanges are applied to the columns on both sides, so
 //    the stored multipliers form L of P A = L U (LAPACK's convention).
-// 2. the right-hand sides get all row swaps at once (B <- P B);
+// 2. the right-hand sides get all row swaps at once (B <- P B): the swaps
+//    are composed into gather indices (piv is overwritten with them) and each
+//    column is permuted through shared memory;
 // 3. L Y = P B and U X = Y by recursive halving: each off-diagonal block is
 //    one GEMM with k up to n/2, only NB x NB diagonal blocks are solved by the
 //    column kernels.  With many right-hand sides (the [A | I] and [D | R | R']
 //    systems of the S-matrix algebra) this moves most of the flops from
 //    rank-NB updates onto large-k GEMMs.
+#include <algorithm>
 #include <functional>
 
 #include "common.cuh"
@@ -188,6 +191,51 @@ lu_rowswap_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int
   }
 }
 
+// The interchanges piv[0..n) composed into one gather: idx[r] = the row of
+// the original right-hand side that ends up in row r (one thread per matrix,
+// indices built in shared memory, then written over piv).
+__global__ void lu_perm_kernel(int* __restrict__ pivg, int n) {
+  extern __shared__ int idx[];
+  int* piv = pivg + (long long)blockIdx.x * n;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) idx[r] = r;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int r = 0; r < n; ++r) {
+      const int p = piv[r];
+      if (p != r) {
+        const int t = idx[r];
+        idx[r] = idx[p];
+        idx[p] = t;
+      }
+    }
+  __syncthreads();
+  for (int r = threadIdx.x; r < n; r += blockDim.x) piv[r] = idx[r];
+}
+
+// B <- P B as a gather with the composed indices: each warp stages one
+// column in shared memory (coalesced read) and writes it back permuted
+// (coalesced write); PERM_CPW columns per warp.
+constexpr int PERM_WARPS = 8, PERM_CPW = 4;
+__global__ void __launch_bounds__(PERM_WARPS * 32)
+lu_gather_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int c_begin, int c_end,
+                 const int* __restrict__ idxg) {
+  extern __shared__ double2 col_sh[];
+  const int nw = blockDim.x >> 5;   // warps (fewer for large n: n doubles2 of shared memory each)
+  const int b = blockIdx.y, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double2* M = Mg + (long long)b * stride;
+  const int* idx = idxg + (long long)b * n;
+  double2* sh = col_sh + (size_t)w * n;
+  for (int t = 0; t < PERM_CPW; ++t) {
+    const int col = c_begin + (blockIdx.x * nw + w) * PERM_CPW + t;
+    if (col >= c_end) break;   // warp-uniform
+    double2* q = M + (long long)col * ld;
+    for (int r = lane; r < n; r += 32) sh[r] = q[r];
+    __syncwarp();
+    for (int r = lane; r < n; r += 32) q[r] = sh[idx[r]];
+    __syncwarp();
+  }
+}
+
 // Upper-triangular solve X = U11^-1 X for rows j..j+jb-1 of the right-hand
 // side columns [c_begin, c_end).
 __global__ void __launch_bounds__(COL_NT)
@@ -283,8 +331,26 @@ int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride,
   // 2. B <- P B
   double2* Bc = M + (long long)n * ld;   // right-hand sides, rows 0..n-1
   {
-    dim3 g(cdiv_up(nrhs, COL_NT), batch);
-    lu_rowswap_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, n, 0, n, n, ncols, piv);
+    const size_t pshm = (size_t)n * sizeof(int);
+    const int pw = (int)std::min<size_t>(PERM_WARPS, (200 * 1024) / ((size_t)n * sizeof(double2)));
+    if (pw < 1) {
+      set_last_error("zgesv: n=%d too large", n);
+      return RCWA_ERR_INVALID;
+    }
+    const size_t gshm = (size_t)pw * n * sizeof(double2);
+    static bool set[64] = {};   // per device: allow the bound once
+    int dev = 0;
+    RCWA_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64 || !set[dev]) {
+      RCWA_CUDA_TRY(cudaFuncSetAttribute(lu_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+      RCWA_CUDA_TRY(cudaFuncSetAttribute(lu_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+      if (dev < 64) set[dev] = true;
+    }
+    lu_perm_kernel<<<batch, 128, pshm, s>>>(piv, n);   // piv now holds the gather indices
+    count_launch();
+    RCWA_LAUNCH_CHECK();
+    dim3 g(cdiv_up(nrhs, pw * PERM_CPW), batch);
+    lu_gather_kernel<<<g, pw * 32, gshm, s>>>(M, ld, stride, n, n, ncols, piv);
     count_launch();
     RCWA_LAUNCH_CHECK();
   }
