@@ -157,6 +157,19 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------- ranks
+def dist_max(x, device):
+    """Max of a per-rank float over all ranks (the timing rule for N > 1);
+    x itself when no process group is running or it has one rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # --------------------------------------------------------------------------- other workloads
 def run_batch_workloads(args):
     """c3 / c4 / c5 (one GPU, rank 0).  One JSON line each; device work is
@@ -306,11 +319,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return dist_max(x, "cuda")
 
     for _ in range(args.warmup):
         step_device()
