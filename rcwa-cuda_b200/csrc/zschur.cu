@@ -6,10 +6,15 @@
 // Iteration (Golub & Van Loan 7.5; LAPACK zlahqr / zlaqr5 rules):
 //  * deflation: the largest k in (l, i] whose subdiagonal passes the
 //    Ahues-Tisseur test is zeroed; an eigenvalue converges when l == i;
+//  * active blocks of AED_MIN rows or more first get aggressive early
+//    deflation (zlaqr3): the trailing NWIN x NWIN window is brought to Schur
+//    form, eigenvalues with a negligible spike entry deflate, the rest of the
+//    window is returned to Hessenberg form and its eigenvalues become shifts;
 //  * active blocks of MS_MIN rows or more get multishift sweeps: NS shifts
-//    (eigenvalues of the trailing NS x NS block, from a small QR run by one
-//    warp; zlaqr0's exceptional shifts every sixth sweep without deflation)
-//    are chased as NS single-shift bulges two positions apart.  Reflectors of
+//    (from the early deflation, else the eigenvalues of the trailing NS x NS
+//    block from a small QR run by one warp; zlaqr0's exceptional shifts every
+//    sixth sweep without deflation) are chased as NS single-shift bulges two
+//    positions apart.  Reflectors of
 //    different bulges in one chase step act on disjoint index pairs, so they
 //    commute: their parameters are computed in parallel (one lane per bulge),
 //    then all left applications run (disjoint rows), then all right
@@ -18,10 +23,10 @@
 //  * smaller active blocks get single-shift sweeps (Wilkinson shift,
 //    exceptional shifts every 10th/20th iteration).
 // Both sweeps are processed window by window: one warp chases inside a
-// diagonal window held in shared memory and logs the reflectors; then the
-// CTA applies the logged reflectors to the rows right of the window, the
-// columns above it and to Z, each thread streaming one row or column through
-// registers (register indices are compile-time, the loops are unrolled).
+// diagonal window held in shared memory and logs the reflectors; the other
+// warps apply the logged reflectors to the columns right of the window, the
+// rows above it and to Z, each thread streaming one row or column through
+// registers.
 #include "common.cuh"
 #include "eig_common.cuh"
 #include "kernels.cuh"
