@@ -89,6 +89,26 @@ typedef struct rcwa_context rcwa_context;
 typedef struct rcwa_geometry rcwa_geometry;
 typedef struct rcwa_server rcwa_server;
 
+/* Layer descriptions for the device-side rasterisers (the reference fills
+ * host grids in main.cpp:48-91).  Coordinates are relative to the cell
+ * centre; shapes are painted in order over the background, cells sampled at
+ * their centres (i + 0.5) L / n. */
+#define RCWA_SHAPE_CIRCLE 1    /* disc of radius a centred at (cx, cy) */
+#define RCWA_SHAPE_RECT 2      /* a x b rectangle centred at (cx, cy) */
+#define RCWA_SHAPE_LINES 3     /* lines along y, width a, centred at x = cx */
+#define RCWA_SHAPE_TRIANGLE 4  /* the reference demo's triangle (main.cpp:51-71): apex up, base = height = a */
+typedef struct rcwa_shape {
+  int kind;
+  double cx, cy, a, b;
+  rcwa_complex eps, mu;
+} rcwa_shape;
+typedef struct rcwa_layer_shapes {
+  rcwa_complex eps_bg, mu_bg;
+  double t;
+  int n_shapes;
+  const rcwa_shape* shapes;
+} rcwa_layer_shapes;
+
 /* ---- context ------------------------------------------------------------ */
 const char* rcwa_last_error(void);
 int rcwa_version(void);
@@ -136,6 +156,19 @@ int rcwa_solve_sweep_device(rcwa_context* ctx, const rcwa_geometry* geom,
                             const rcwa_source* sources, int n_sources, int precision,
                             double* R_dev, double* T_dev, double* tot_dev,
                             uint32_t* status_dev);
+
+/* Device-side rasterisers.  rcwa_rasterize writes the er/ur grids of nl
+ * layers ([layer][iy][ix], device pointers) and, if t_dev is not NULL, the
+ * thicknesses; asynchronous on the context stream.  The grids equal the
+ * host builders' of rcwa_b200.configs bit for bit.
+ * rcwa_geometry_create_shapes rasterises into temporary device grids and
+ * builds the geometry from them (no host grids at all). */
+int rcwa_rasterize(rcwa_context* ctx, int nx, int ny, double lx, double ly, int nl,
+                   const rcwa_layer_shapes* layers, rcwa_complex* er_dev, rcwa_complex* ur_dev,
+                   double* t_dev);
+int rcwa_geometry_create_shapes(rcwa_context* ctx, int nx, int ny, double lx, double ly, int nl,
+                                const rcwa_layer_shapes* layers, const rcwa_params* params,
+                                rcwa_geometry** out);
 
 /* ---- batches and serving ------------------------------------------------
  * The reference solves one problem per call (main.cpp:111-191); these run

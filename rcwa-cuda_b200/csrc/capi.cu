@@ -231,6 +231,40 @@ int rcwa_solve(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_source* so
   return rcwa_solve_sweep(ctx, stack, source, 1, params, precision, out);
 }
 
+int rcwa_rasterize(rcwa_context* ctx, int nx, int ny, double lx, double ly, int nl,
+                   const rcwa_layer_shapes* layers, rcwa_complex* er_dev, rcwa_complex* ur_dev,
+                   double* t_dev) {
+  CHECK_ARG(ctx && (nl == 0 || (layers && er_dev && ur_dev)), "NULL argument");
+  CHECK_ARG(nx > 0 && ny > 0 && nl >= 0 && lx > 0 && ly > 0, "bad grid");
+  for (int l = 0; l < nl; ++l) CHECK_ARG(layers[l].n_shapes >= 0 && (layers[l].n_shapes == 0 || layers[l].shapes), "bad layer");
+  RCWA_CUDA_TRY(cudaSetDevice(ctx->device));
+  return rasterize(ctx, nx, ny, lx, ly, nl, layers, (double2*)er_dev, (double2*)ur_dev, t_dev);
+}
+
+int rcwa_geometry_create_shapes(rcwa_context* ctx, int nx, int ny, double lx, double ly, int nl,
+                                const rcwa_layer_shapes* layers, const rcwa_params* params,
+                                rcwa_geometry** out) {
+  CHECK_ARG(ctx && out && (nl == 0 || layers), "NULL argument");
+  CHECK_ARG(nx > 0 && ny > 0 && nl >= 0 && lx > 0 && ly > 0, "bad grid");
+  int rc = check_params(params);
+  if (rc) return rc;
+  RCWA_CUDA_TRY(cudaSetDevice(ctx->device));
+  const size_t G = (size_t)nx * ny;
+  char* buf = nullptr;
+  const size_t bytes = 2 * (size_t)(nl > 0 ? nl : 1) * G * sizeof(double2) + (size_t)(nl + 1) * sizeof(double) + 512;
+  RCWA_CUDA_TRY(cudaMallocAsync((void**)&buf, bytes, ctx->stream));
+  double2* er = (double2*)buf;
+  double2* ur = er + (size_t)nl * G;
+  double* t = (double*)(ur + (size_t)nl * G);
+  rc = rasterize(ctx, nx, ny, lx, ly, nl, layers, er, ur, t);
+  if (!rc) {
+    rcwa_stack st{nx, ny, nl, lx, ly, (const rcwa_complex*)er, (const rcwa_complex*)ur, t};
+    rc = rcwa_geometry_create(ctx, &st, params, 1, out);   // reads the grids in place, synchronises
+  }
+  cudaFreeAsync(buf, ctx->stream);
+  return rc;
+}
+
 int rcwa_solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_source* sources,
                      const rcwa_params* params, int precision, rcwa_result* out) {
   CHECK_ARG(ctx && stacks && sources && params && out, "NULL argument");

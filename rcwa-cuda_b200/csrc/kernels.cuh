@@ -119,10 +119,14 @@ int port_smatrix(cudaStream_t s, int B, const ModeDims& d, int side, double2 er,
                  long long sS, int bd);
 // Source, fields and efficiencies (rcwa.cpp:469-585) from S_global's S11/S21
 // (full n x n blocks, or compact: only the two source columns, n x 2).
+// map / oidx / ustatus (device, may be null): B source records that share
+// solves -- record e uses the S columns and wave vectors of solve map[e],
+// writes output row oidx[e] and takes the solve's status ustatus[map[e]].
 int efficiencies(cudaStream_t s, int B, const ModeDims& d, const SourceDev* src_dev,
                  double2 ur_ref, double2 ur_trn, const WaveVecs& w, const double2* S11,
                  const double2* S21, long long sS, int compact, double* R, double* T, double* tot,
-                 uint32_t* status);
+                 uint32_t* status, const int* map = nullptr, const int* oidx = nullptr,
+                 const uint32_t* ustatus = nullptr);
 // C = beta C + alpha (X M) (side 0) or (M X) (side 1) [+ I], X in BD form.
 int bd_apply(cudaStream_t s, int side, int N, int rows, int cols, const double2* X, long long sX,
              const double2* M, int ldm, long long sM, double2* C, int ldc, long long sC,

@@ -489,18 +489,27 @@ __device__ void normalize3(double2 v[3]) {
     for (int k = 0; k < 3; ++k) v[k] = cmk(v[k].x / nrm, v[k].y / nrm);
 }
 
+// Block e computes the efficiencies of source record srcs[e] from the
+// S-matrix columns and wave vectors of solve u = map[e] (map null: u = e) and
+// writes them to row o = oidx[e] of the outputs (oidx null: o = e).  With
+// ustatus, status[o] = ustatus[u] | flags (sources that share one solve);
+// otherwise the flags are ORed into status[o].
 __global__ void efficiencies_kernel(int N, const SourceDev* __restrict__ srcs, double2 ur_ref,
                                     double2 ur_trn, WaveVecs w, const double2* __restrict__ S11g,
                                     const double2* __restrict__ S21g, long long sS, int compact,
-                                    double* __restrict__ Rg, double* __restrict__ Tg,
-                                    double* __restrict__ tot, uint32_t* __restrict__ status) {
-  const int b = blockIdx.x;
+                                    const int* __restrict__ map, const int* __restrict__ oidx,
+                                    const uint32_t* __restrict__ ustatus, double* __restrict__ Rg,
+                                    double* __restrict__ Tg, double* __restrict__ tot,
+                                    uint32_t* __restrict__ status) {
+  const int e = blockIdx.x;
+  const int b = map ? map[e] : e;         // the solve whose S-matrix and wave vectors are used
+  const long long ob = oidx ? oidx[e] : e; // the output row
   const int n = 2 * N;
   __shared__ double2 s_pol[2];
   __shared__ double red[2][32];
   const double2* ki = w.kinc + (long long)b * 4;
   if (threadIdx.x == 0) {
-    const SourceDev sv = srcs[b];
+    const SourceDev sv = srcs[e];
     double2 k[3] = {ki[0], ki[1], ki[2]};
     double2 te[3], tm[3], pol[3];
     if (fabs(sv.theta) < 1e-6) {                       // :483-486
@@ -530,6 +539,7 @@ __global__ void efficiencies_kernel(int N, const SourceDev* __restrict__ srcs, d
   bool bad = false;
   for (int m = threadIdx.x; m < N; m += blockDim.x) {
     const long long o = (long long)b * N + m;
+    const long long oo = ob * N + m;
     const double2 kx = w.Kx[o], ky = w.Ky[o];
     // r = S11 csrc (:535), r_z (:541)
     double2 rx = cadd(cmul(S11[(long long)src0 * n + m], c1), cmul(S11[(long long)src1 * n + m], c2));
@@ -542,8 +552,8 @@ __global__ void efficiencies_kernel(int N, const SourceDev* __restrict__ srcs, d
     const double tt = cabs2(tx) + cabs2(ty) + cabs2(tz);
     const double R = (cdiv(cneg(w.Kzr[o]), ur_ref).x / den) * rr;      // :576
     const double T = (cdiv(w.Kzt[o], ur_trn).x / den) * tt;             // :582
-    Rg[o] = R;   // column-major Q x P: index p*Q + q == m
-    Tg[o] = T;
+    Rg[oo] = R;   // column-major Q x P: index p*Q + q == m
+    Tg[oo] = T;
     rsum += R;
     tsum += T;
     if (!isfinite(R) || !isfinite(T)) bad = true;
@@ -562,9 +572,12 @@ __global__ void efficiencies_kernel(int N, const SourceDev* __restrict__ srcs, d
       a += red[0][k];
       c += red[1][k];
     }
-    tot[(long long)b * 2] = a;
-    tot[(long long)b * 2 + 1] = c;
-    if (bad) atomicOr(status + b, (unsigned)ST_NONFINITE);
+    tot[ob * 2] = a;
+    tot[ob * 2 + 1] = c;
+    if (ustatus)
+      status[ob] = ustatus[b] | (bad ? (uint32_t)ST_NONFINITE : 0u);
+    else if (bad)
+      atomicOr(status + ob, (unsigned)ST_NONFINITE);
   }
 }
 
@@ -725,9 +738,10 @@ int port_smatrix(cudaStream_t s, int B, const ModeDims& d, int side, double2 er,
 int efficiencies(cudaStream_t s, int B, const ModeDims& d, const SourceDev* src_dev,
                  double2 ur_ref, double2 ur_trn, const WaveVecs& w, const double2* S11,
                  const double2* S21, long long sS, int compact, double* R, double* T, double* tot,
-                 uint32_t* status) {
-  efficiencies_kernel<<<B, 256, 0, s>>>(d.N, src_dev, ur_ref, ur_trn, w, S11, S21, sS, compact, R, T,
-                                         tot, status);
+                 uint32_t* status, const int* map, const int* oidx, const uint32_t* ustatus) {
+  if (B <= 0) return RCWA_OK;
+  efficiencies_kernel<<<B, 256, 0, s>>>(d.N, src_dev, ur_ref, ur_trn, w, S11, S21, sS, compact, map,
+                                         oidx, ustatus, R, T, tot, status);
   count_launch();
   RCWA_LAUNCH_CHECK();
   return RCWA_OK;

@@ -17,6 +17,9 @@
 #include <algorithm>
 #include <cstring>
 
+#include <map>
+#include <tuple>
+
 #include "solver.cuh"
 
 namespace rcwa {
@@ -684,7 +687,7 @@ Layers layers_of(const rcwa_geometry* g) {
 // One chunk of B solves on the layer set g; hsrc: host [B] sources with
 // their lattice periods.
 int sweep_chunk_layers(rcwa_context* ctx, const Layers& g, const SourceDev* hsrc, int B, double* R,
-                       double* T, double* tot, uint32_t* status) {
+                       double* T, double* tot, uint32_t* status, const ShareMap* sh) {
   cudaStream_t s = ctx->stream;
   const ModeDims& d = g.d;
   const int n = d.n;
@@ -802,6 +805,9 @@ int sweep_chunk_layers(rcwa_context* ctx, const Layers& g, const SourceDev* hsrc
                            pl.s0, pl.s1, pl.piv, pl.st, status)))
     return rc;
   // efficiencies (main.cpp:182-191)
+  if (sh)   // sources sharing these solves (polarisation variants)
+    return efficiencies(s, sh->n, d, sh->src, g.ur_ref, g.ur_trn, pl.wv, S11E, S21E, 2LL * n, 1, sh->R,
+                        sh->T, sh->tot, sh->status, sh->map, sh->oidx, status);
   return efficiencies(s, B, d, pl.src, g.ur_ref, g.ur_trn, pl.wv, S11E, S21E, 2LL * n, 1, R, T,
                       tot, status);
 }
@@ -841,16 +847,86 @@ int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* s
   int chunk = (int)std::max<size_t>(1, budget / per);
   chunk = std::min(chunk, B);
   const Layers G = layers_of(g);
-  std::vector<SourceDev> hs(chunk);
-  for (int b0 = 0; b0 < B; b0 += chunk) {
-    const int bc = std::min(chunk, B - b0);
-    const long long N = d.N;
-    for (int b = 0; b < bc; ++b) {
-      const rcwa_source& q = sources[b0 + b];
-      hs[b] = SourceDev{q.lambda0, q.theta, q.phi, q.pte, q.ptm, g->lx, g->ly};
+  // sources that differ only in polarisation share one solve: the S-matrix
+  // and wave vectors depend on (lambda0, theta, phi) alone; only the source
+  // vector of the efficiencies (rcwa.cpp:469-523) sees pte/ptm
+  std::map<std::tuple<double, double, double>, int> key;
+  std::vector<int> uof(B);
+  std::vector<int> firsts;
+  for (int b = 0; b < B; ++b) {
+    const auto k = std::make_tuple(sources[b].lambda0, sources[b].theta, sources[b].phi);
+    auto it = key.find(k);
+    if (it == key.end()) {
+      it = key.emplace(k, (int)firsts.size()).first;
+      firsts.push_back(b);
     }
-    int rc = sweep_chunk_layers(ctx, G, hs.data(), bc, R + b0 * N, T + b0 * N, tot + 2LL * b0, status + b0);
-    if (rc) return rc;
+    uof[b] = it->second;
+  }
+  const int U = (int)firsts.size();
+  const long long N = d.N;
+  if (U == B) {
+    std::vector<SourceDev> hs(chunk);
+    for (int b0 = 0; b0 < B; b0 += chunk) {
+      const int bc = std::min(chunk, B - b0);
+      for (int b = 0; b < bc; ++b) {
+        const rcwa_source& q = sources[b0 + b];
+        hs[b] = SourceDev{q.lambda0, q.theta, q.phi, q.pte, q.ptm, g->lx, g->ly};
+      }
+      int rc = sweep_chunk_layers(ctx, G, hs.data(), bc, R + b0 * N, T + b0 * N, tot + 2LL * b0, status + b0);
+      if (rc) return rc;
+    }
+  } else {
+    // solves for the U distinct (lambda0, theta, phi); efficiencies for all B
+    std::vector<std::vector<int>> members(U);
+    for (int b = 0; b < B; ++b) members[uof[b]].push_back(b);
+    char* buf = nullptr;
+    const size_t bytes = (size_t)B * (sizeof(SourceDev) + 2 * sizeof(int)) + (size_t)U * sizeof(uint32_t) + 1024;
+    RCWA_CUDA_TRY(cudaMallocAsync((void**)&buf, bytes, ctx->stream));
+    struct Free {
+      char* p;
+      cudaStream_t s;
+      ~Free() { cudaFreeAsync(p, s); }
+    } free_buf{buf, ctx->stream};
+    SourceDev* esrc = (SourceDev*)buf;
+    int* emap = (int*)(esrc + B);
+    int* eoidx = emap + B;
+    uint32_t* ust = (uint32_t*)(eoidx + B);
+    std::vector<std::vector<SourceDev>> keep_src;   // host copies live until the end
+    std::vector<std::vector<int>> keep_idx;
+    for (int u0 = 0; u0 < U; u0 += chunk) {
+      const int uc = std::min(chunk, U - u0);
+      std::vector<SourceDev> hs(uc), es;
+      std::vector<int> em, eo;
+      for (int u = 0; u < uc; ++u) {
+        const rcwa_source& q = sources[firsts[u0 + u]];
+        hs[u] = SourceDev{q.lambda0, q.theta, q.phi, q.pte, q.ptm, g->lx, g->ly};
+        for (int b : members[u0 + u]) {
+          const rcwa_source& r = sources[b];
+          es.push_back(SourceDev{r.lambda0, r.theta, r.phi, r.pte, r.ptm, g->lx, g->ly});
+          em.push_back(u);
+          eo.push_back(b);
+        }
+      }
+      const int ne = (int)es.size();
+      RCWA_CUDA_TRY(cudaMemcpyAsync(esrc, es.data(), ne * sizeof(SourceDev), cudaMemcpyHostToDevice, ctx->stream));
+      RCWA_CUDA_TRY(cudaMemcpyAsync(emap, em.data(), ne * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+      RCWA_CUDA_TRY(cudaMemcpyAsync(eoidx, eo.data(), ne * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+      ShareMap sh;
+      sh.n = ne;
+      sh.src = esrc;
+      sh.map = emap;
+      sh.oidx = eoidx;
+      sh.R = R;
+      sh.T = T;
+      sh.tot = tot;
+      sh.status = status;
+      int rc = sweep_chunk_layers(ctx, G, hs.data(), uc, nullptr, nullptr, nullptr, ust, &sh);
+      if (rc) return rc;
+      keep_src.push_back(std::move(es));
+      keep_idx.push_back(std::move(em));
+      keep_idx.push_back(std::move(eo));
+      RCWA_CUDA_TRY(cudaStreamSynchronize(ctx->stream));   // the staging arrays are reused
+    }
   }
   if (tc_err) {
     int h = 0;

@@ -74,10 +74,26 @@ struct Layers {
   int items(int l, int B) const { return nb ? (nb[l] < B ? nb[l] : B) : B; }
 };
 Layers layers_of(const rcwa_geometry* g);
+// Source records that share the chunk's solves (sources that differ only in
+// polarisation): record e takes the S-matrix of solve map[e] and writes
+// output row oidx[e].  All pointers are device pointers.
+struct ShareMap {
+  int n = 0;
+  const SourceDev* src = nullptr;
+  const int* map = nullptr;
+  const int* oidx = nullptr;
+  double *R = nullptr, *T = nullptr, *tot = nullptr;
+  uint32_t* status = nullptr;
+};
 // One chunk of B solves (device outputs R/T [B][N], tot [B][2], status [B]);
-// hsrc: host array of the B sources with their lattice periods.
+// hsrc: host array of the B sources with their lattice periods.  With sh,
+// the efficiencies are computed for sh's records instead (R, T, tot unused;
+// status receives the B solves' flags).
 int sweep_chunk_layers(rcwa_context* ctx, const Layers& g, const SourceDev* hsrc, int B, double* R,
-                       double* T, double* tot, uint32_t* status);
+                       double* T, double* tot, uint32_t* status, const ShareMap* sh = nullptr);
+// Device-side rasterisers (raster.cu).
+int rasterize(rcwa_context* ctx, int nx, int ny, double lx, double ly, int nl,
+              const rcwa_layer_shapes* layers, double2* er, double2* ur, double* t_dev);
 // n unrelated problems, grouped by shape into batched solves (batch.cu);
 // max_group > 0 caps the solves per batched launch sequence.
 int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_source* sources,

@@ -61,6 +61,19 @@ class CParams(C.Structure):
                 ("er_trn", CComplex), ("ur_trn", CComplex)]
 
 
+class CShape(C.Structure):
+    _fields_ = [("kind", C.c_int), ("cx", C.c_double), ("cy", C.c_double), ("a", C.c_double),
+                ("b", C.c_double), ("eps", CComplex), ("mu", CComplex)]
+
+
+class CLayerShapes(C.Structure):
+    _fields_ = [("eps_bg", CComplex), ("mu_bg", CComplex), ("t", C.c_double), ("n_shapes", C.c_int),
+                ("shapes", C.c_void_p)]
+
+
+SHAPE_CIRCLE, SHAPE_RECT, SHAPE_LINES, SHAPE_TRIANGLE = 1, 2, 3, 4
+
+
 class CResult(C.Structure):
     _fields_ = [("R", C.c_void_p), ("T", C.c_void_p), ("R_tot", C.c_double),
                 ("T_tot", C.c_double), ("status", C.c_uint32)]
@@ -102,6 +115,10 @@ _SIGS = {
     "rcwa_eig_noalloc": ([C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_lu_solve": ([_VP, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_gemm": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, C.c_int], C.c_int),
+    "rcwa_rasterize": ([_VP, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.POINTER(CLayerShapes),
+                        _VP, _VP, _VP], C.c_int),
+    "rcwa_geometry_create_shapes": ([_VP, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                     C.POINTER(CLayerShapes), C.POINTER(CParams), C.POINTER(_VP)], C.c_int),
     "rcwa_solve_batch": ([_VP, C.c_int, C.POINTER(CStack), C.POINTER(CSource), C.POINTER(CParams),
                           C.c_int, C.POINTER(CResult)], C.c_int),
     "rcwa_server_create": ([C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_VP)], C.c_int),
@@ -418,6 +435,35 @@ class Context:
         _check(self.lib.rcwa_gemm(self.h, m, n, k, b, _ptr(Af), _ptr(Bf), _ptr(Cf), precision))
         Cm = Cf.transpose(0, 2, 1)
         return Cm[0] if single else Cm
+
+    # ---- device-side rasterisers --------------------------------------------
+    @staticmethod
+    def _layers(layers):
+        """layers: [(eps_bg, mu_bg, t, [(kind, cx, cy, a, b, eps, mu), ...]), ...]"""
+        cc = lambda z: CComplex(float(np.real(z)), float(np.imag(z)))
+        keep = []
+        arr = (CLayerShapes * max(1, len(layers)))()
+        for i, (eb, mb, t, shapes) in enumerate(layers):
+            sa = (CShape * max(1, len(shapes)))()
+            for j, (k, cx, cy, a, b, e, m) in enumerate(shapes):
+                sa[j] = CShape(int(k), float(cx), float(cy), float(a), float(b), cc(e), cc(m))
+            keep.append(sa)
+            arr[i] = CLayerShapes(cc(eb), cc(mb), float(t), len(shapes), C.cast(sa, C.c_void_p).value)
+        return arr, keep
+
+    def rasterize(self, nx, ny, lx, ly, layers, er_ptr, ur_ptr, t_ptr=None):
+        """``rcwa_rasterize`` into device buffers (e.g. torch tensors' data_ptr())."""
+        arr, keep = self._layers(layers)
+        _check(self.lib.rcwa_rasterize(self.h, nx, ny, lx, ly, len(layers), arr, er_ptr, ur_ptr, t_ptr))
+        del keep
+
+    def geometry_create_shapes(self, nx, ny, lx, ly, layers, p: ParamSpec):
+        arr, keep = self._layers(layers)
+        h = C.c_void_p()
+        _check(self.lib.rcwa_geometry_create_shapes(self.h, nx, ny, lx, ly, len(layers), arr,
+                                                    C.byref(c_params(p)), C.byref(h)))
+        del keep
+        return h
 
     # ---- batches of unrelated problems --------------------------------------
     def solve_batch(self, problems: Sequence[Problem], precision: int = PREC_FP64,

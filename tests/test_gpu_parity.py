@@ -312,3 +312,21 @@ def test_golden_fixtures(ctx, name):
     assert np.abs(T - z["T"]).max() <= TOL_RT
     assert np.abs(Rt - z["R_tot"]).max() <= TOL_RT
     assert np.abs(Tt - z["T_tot"]).max() <= TOL_RT
+
+
+def test_polarisation_variants_share_solves(ctx):
+    """Sources that differ only in (pte, ptm) share one S-matrix solve; every
+    source still gets its own efficiencies in its own output row."""
+    import dataclasses
+    pb0 = _small_layer_problem()
+    mk = lambda lam, th, ph, te, tm: C.SourceSpec(lam, math.radians(th), math.radians(ph), te, tm)
+    srcs = [mk(600.0, 17.0, 11.0, 1.0, 0.0), mk(650.0, 5.0, 0.0, 0.0, 1.0), mk(600.0, 17.0, 11.0, 0.0, 1.0),
+            mk(600.0, 17.0, 11.0, 0.6, 0.8), mk(650.0, 5.0, 0.0, 1.0, 0.0)]
+    pb = dataclasses.replace(pb0, sources=srcs)
+    R, T, Rt, Tt, st = ctx.solve_sweep(pb)
+    assert not st.any()
+    for i in range(len(srcs)):
+        ref = oracle_solve(pb, i)
+        _assert_parity(R[i], T[i], Rt[i], Tt[i], ref)
+        R1, T1, Rt1, Tt1, st1 = ctx.solve_sweep(pb, sources=[srcs[i]])
+        assert np.abs(R1[0] - R[i]).max() <= 1e-13 and abs(Tt1[0] - Tt[i]) <= 1e-13
