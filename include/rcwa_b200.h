@@ -146,6 +146,20 @@ int rcwa_solve_sweep(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_sour
  * stream: use a geometry only with the context that created it. */
 int rcwa_geometry_create(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_params* params,
                          int stack_on_device, rcwa_geometry** out);
+/* rcwa_geometry_create with option flags (0 = rcwa_geometry_create).
+ * RCWA_GEOM_LI_RULE: Li's factorization rule for crossed gratings (J. Opt.
+ * Soc. Am. A 14, 2758 (1997)) in place of the reference's Laurent rule where
+ * eps / mu multiply the in-plane field components (Q_i: E_x, E_y; P_i: H_x,
+ * H_y of rcwa.cpp:273-285): eps_xx = [[ [[eps]]_x ]]_y, the inverse of the 1-D
+ * Toeplitz matrix of 1/eps along every grid row, convolved along y, and
+ * eps_yy with the axes swapped.  erc^-1 / urc^-1 (rcwa.cpp:267-281) keep the
+ * Laurent rule.  Converges much faster for TM light on high-contrast and
+ * metallic lamellar gratings; the reference has no such option, so its
+ * results differ by the truncation error.  Returns RCWA_ERR_NUMERIC if a grid
+ * value is 0 or a line's 1/eps Toeplitz matrix is singular. */
+#define RCWA_GEOM_LI_RULE 1u
+int rcwa_geometry_create_ex(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_params* params,
+                            int stack_on_device, unsigned flags, rcwa_geometry** out);
 /* Releases the geometry in stream order on its context's stream (work already
  * enqueued that reads it completes first); does not block the host. */
 int rcwa_geometry_destroy(rcwa_geometry* geom);

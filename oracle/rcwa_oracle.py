@@ -52,7 +52,7 @@ __all__ = [
     "smatrix_init", "smatrix_layer", "smatrix_reflection",
     "smatrix_transmission", "redheffer_product", "source_mode_coeff",
     "reflected_field", "transmitted_field", "diffraction_efficiencies",
-    "solve", "Stack", "Source", "Params", "Results", "SMatrix",
+    "solve", "Stack", "Source", "Params", "Results", "SMatrix", "li_conv_mat",
 ]
 
 
@@ -153,6 +153,45 @@ def conv_mat(field, layer, Nx, Ny, Nx_harmonics, Ny_harmonics):
     return C
 
 
+def _dft_1d(lines, n, K):
+    """Coefficients k = -K..K of the 1-D DFT of each row of ``lines`` (last axis,
+    length n), divided by n; 0 where k + n//2 lies outside [0, n), the range
+    rule of rcwa.cpp:71-73 applied to one axis."""
+    F = np.fft.fft(lines, axis=-1) / float(n)
+    k = np.arange(-K, K + 1)
+    out = F[..., k % n]
+    out[..., (k + n // 2 < 0) | (k + n // 2 >= n)] = 0.0
+    return out
+
+
+def li_conv_mat(field, layer, Nx, Ny, Nx_harmonics, Ny_harmonics, axis):
+    """Li's factorization rule for crossed gratings (L. Li, J. Opt. Soc. Am. A
+    14, 2758 (1997)) -- an option the reference does not have; its ConvMat
+    (rcwa.cpp:6-82) is the Laurent rule everywhere.
+
+    axis "x" gives eps_xx = [[ [[eps]]_x ]]_y: along each grid row (fixed y) the
+    1-D Toeplitz matrix of 1/eps in the x harmonics is inverted (inverse rule,
+    x being normal to the walls that the field component crosses), and the
+    inverses are then convolved along y (Laurent rule).  axis "y" swaps the two
+    axes.  The mode index is m = p*Q + q (x slow) as in conv_mat.
+    """
+    F = np.asarray(field, dtype=np.complex128)[layer * Nx * Ny:(layer + 1) * Nx * Ny].reshape(Ny, Nx)
+    P = 2 * Nx_harmonics + 1
+    Q = 2 * Ny_harmonics + 1
+    if axis == "x":
+        lines, na, nb, Pa, Pb = 1.0 / F, Nx, Ny, P, Q
+    else:
+        lines, na, nb, Pa, Pb = (1.0 / F).T, Ny, Nx, Q, P
+    a = _dft_1d(lines, na, Pa - 1)                        # [nb][2Pa-1]
+    d = np.arange(Pa)[:, None] - np.arange(Pa)[None, :] + Pa - 1
+    eye = np.eye(Pa, dtype=np.complex128)
+    M = np.stack([_lu_solve(a[i][d], eye) for i in range(nb)])   # [nb][Pa][Pa]
+    c = _dft_1d(np.moveaxis(M, 0, -1), nb, Pb - 1)        # [Pa][Pa][2Pb-1]
+    m = np.arange(P * Q)
+    pa, pb = (m // Q, m % Q) if axis == "x" else (m % Q, m // Q)
+    return c[pa[:, None], pa[None, :], pb[:, None] - pb[None, :] + Pb - 1]
+
+
 def compute_wave_vectors(Lx, Ly, source: Source, params: Params):
     """rcwa.cpp:85-160 -> (k_inc[3], Kx, Ky, Kz_ref, Kz_trn), vectors of length PQ."""
     n_inc = np.sqrt(complex(params.er_ref) * complex(params.ur_ref))   # std::sqrt, :91
@@ -208,23 +247,29 @@ def smatrix_init(Nx_harmonics, Ny_harmonics):
     return SMatrix(Z.copy(), I.copy(), I.copy(), Z.copy())
 
 
-def layer_pq(erc, urc, Kx, Ky):
-    """rcwa.cpp:262-286 -> (P_i, Q_i)."""
+def layer_pq(erc, urc, Kx, Ky, li=None):
+    """rcwa.cpp:262-286 -> (P_i, Q_i).
+
+    ``li`` = (eps_xx, eps_yy, mu_xx, mu_yy) from li_conv_mat replaces erc / urc
+    where they multiply the in-plane field components (Q: E_x, E_y; P: H_x,
+    H_y); erc^-1 / urc^-1 (the z components) keep the Laurent rule.
+    """
+    exx, eyy, mxx, myy = (erc, erc, urc, urc) if li is None else li
     N = Kx.size
     DKx, DKy = np.diag(Kx), np.diag(Ky)
     erc_inv_Kx = _lu_solve(erc, DKx)                                    # :267
     erc_inv_Ky = _lu_solve(erc, DKy)                                    # :270
     P = np.zeros((2 * N, 2 * N), dtype=np.complex128)
     P[:N, :N] = Kx[:, None] * erc_inv_Ky                                # :273
-    P[:N, N:] = urc - Kx[:, None] * erc_inv_Kx                          # :274
-    P[N:, :N] = Ky[:, None] * erc_inv_Ky - urc                          # :275
+    P[:N, N:] = myy - Kx[:, None] * erc_inv_Kx                          # :274
+    P[N:, :N] = Ky[:, None] * erc_inv_Ky - mxx                          # :275
     P[N:, N:] = (-Ky)[:, None] * erc_inv_Kx                             # :276
     urc_inv_Kx = _lu_solve(urc, DKx)                                    # :280
     urc_inv_Ky = _lu_solve(urc, DKy)                                    # :281
     Qm = np.zeros((2 * N, 2 * N), dtype=np.complex128)
     Qm[:N, :N] = Kx[:, None] * urc_inv_Ky                               # :282
-    Qm[:N, N:] = erc - Kx[:, None] * urc_inv_Kx                         # :283
-    Qm[N:, :N] = Ky[:, None] * urc_inv_Ky - erc                         # :284
+    Qm[:N, N:] = eyy - Kx[:, None] * urc_inv_Kx                         # :283
+    Qm[N:, :N] = Ky[:, None] * urc_inv_Ky - exx                         # :284
     Qm[N:, N:] = (-Ky)[:, None] * urc_inv_Kx                            # :285
     return P, Qm
 
@@ -247,12 +292,13 @@ def layer_smatrix_from_modes(W, lam, Qm, W0, V0, k0, t):
     return SMatrix(S11, S12, S12.copy(), S11.copy())                    # :351
 
 
-def smatrix_layer(erc, urc, Kx, Ky, W0, V0, k0, t, eig=None):
+def smatrix_layer(erc, urc, Kx, Ky, W0, V0, k0, t, eig=None, li=None):
     """rcwa.cpp:254-352 -- one layer's (symmetric) S-matrix.
 
-    ``eig`` may replace the eigensolver (rcwa.cpp:298) to test basis invariance.
+    ``eig`` may replace the eigensolver (rcwa.cpp:298) to test basis invariance;
+    ``li`` selects Li's factorization rule (see layer_pq).
     """
-    P, Qm = layer_pq(erc, urc, Kx, Ky)
+    P, Qm = layer_pq(erc, urc, Kx, Ky, li)
     Omega2 = P @ Qm                                                     # :288
     if eig is None:
         lam2, W = sla.eig(Omega2, check_finite=False)                   # :298-306
@@ -376,27 +422,40 @@ def diffraction_efficiencies(params: Params, r, t, k_inc, Kz_ref, Kz_trn) -> Res
 # ----------------------------------------------------------------------------
 # solve orchestration (main.cpp:111-191)
 # ----------------------------------------------------------------------------
-def conv_mats(stack: Stack, params: Params):
-    """main.cpp:125-138: erc/urc per layer."""
+def conv_mats(stack: Stack, params: Params, rule: str = "laurent"):
+    """main.cpp:125-138: erc/urc per layer.  rule "li" adds a third list of
+    per-layer (eps_xx, eps_yy, mu_xx, mu_yy) (li_conv_mat)."""
     erc, urc = [], []
+    h = (stack.Nx, stack.Ny, params.Nx_harmonics, params.Ny_harmonics)
     for l in range(stack.num_layers):
-        erc.append(conv_mat(stack.er, l, stack.Nx, stack.Ny, params.Nx_harmonics, params.Ny_harmonics))
-        urc.append(conv_mat(stack.ur, l, stack.Nx, stack.Ny, params.Nx_harmonics, params.Ny_harmonics))
-    return erc, urc
+        erc.append(conv_mat(stack.er, l, *h))
+        urc.append(conv_mat(stack.ur, l, *h))
+    if rule == "laurent":
+        return erc, urc
+    if rule != "li":
+        raise ValueError(f"unknown factorization rule {rule!r}")
+    li = [(li_conv_mat(stack.er, l, *h, "x"), li_conv_mat(stack.er, l, *h, "y"),
+           li_conv_mat(stack.ur, l, *h, "x"), li_conv_mat(stack.ur, l, *h, "y"))
+          for l in range(stack.num_layers)]
+    return erc, urc, li
 
 
-def solve(stack: Stack, source: Source, params: Params, convs=None, return_smatrix=False):
+def solve(stack: Stack, source: Source, params: Params, convs=None, return_smatrix=False,
+          rule: str = "laurent"):
     """main.cpp:111-191: the reference's end-to-end solve for one source.
 
-    ``convs`` optionally passes precomputed (erc, urc) lists (they depend on the
-    grid and harmonics only, not on the source).
+    ``convs`` optionally passes precomputed conv_mats output (it depends on the
+    grid and harmonics only, not on the source); a 3-tuple carries Li's
+    matrices and selects that rule, as does ``rule="li"``.
     """
-    erc, urc = convs if convs is not None else conv_mats(stack, params)
+    convs = convs if convs is not None else conv_mats(stack, params, rule)
+    erc, urc = convs[0], convs[1]
+    li = convs[2] if len(convs) > 2 else [None] * stack.num_layers
     k_inc, Kx, Ky, Kz_ref, Kz_trn = compute_wave_vectors(stack.Lx, stack.Ly, source, params)
     W0, V0 = gap_medium(Kx, Ky)
     S_dev = smatrix_init(params.Nx_harmonics, params.Ny_harmonics)
     for l in range(stack.num_layers):
-        S_l = smatrix_layer(erc[l], urc[l], Kx, Ky, W0, V0, source.k0, float(stack.t[l]))
+        S_l = smatrix_layer(erc[l], urc[l], Kx, Ky, W0, V0, source.k0, float(stack.t[l]), li=li[l])
         S_dev = redheffer_product(S_dev, S_l)
     S_ref, W_ref = smatrix_reflection(params, Kx, Ky, Kz_ref, W0, V0)
     S_trn, W_trn = smatrix_transmission(params, Kx, Ky, Kz_trn, W0, V0)

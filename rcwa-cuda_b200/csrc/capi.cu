@@ -140,14 +140,20 @@ int rcwa_context_kernel_launches(rcwa_context* c, uint64_t* count) {
 
 int rcwa_geometry_create(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_params* params,
                          int stack_on_device, rcwa_geometry** out) {
+  return rcwa_geometry_create_ex(ctx, stack, params, stack_on_device, 0u, out);
+}
+
+int rcwa_geometry_create_ex(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_params* params,
+                            int stack_on_device, unsigned flags, rcwa_geometry** out) {
   CHECK_ARG(ctx && out, "NULL argument");
+  CHECK_ARG((flags & ~RCWA_GEOM_LI_RULE) == 0u, "unknown geometry flags");
   int rc = check_stack(stack);
   if (rc) return rc;
   if ((rc = check_params(params))) return rc;
   RCWA_CUDA_TRY(cudaSetDevice(ctx->device));
   rcwa_geometry* g = new (std::nothrow) rcwa_geometry();
   if (!g) return RCWA_ERR_NOMEM;
-  rc = geometry_build(ctx, g, stack, params, stack_on_device);
+  rc = geometry_build(ctx, g, stack, params, stack_on_device, flags);
   if (rc) {
     geometry_free(g);
     delete g;

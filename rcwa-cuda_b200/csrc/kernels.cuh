@@ -71,6 +71,12 @@ struct ModeDims {
 int convmat(cudaStream_t s, const double2* grids, int nl, int nx, int ny, const ModeDims& d,
             double2* out, double2* scratch);
 size_t convmat_scratch_bytes(int nl, int nx, int ny, const ModeDims& d);
+// Li's factorization rule: out[l] = eps_xx (axis_y = 0) or eps_yy (axis_y = 1)
+// of `nl` layer grids, N x N.  *bad |= 1 for a zero / non-finite grid value,
+// |= 2 for a singular line Toeplitz matrix.
+int li_convmat(cudaStream_t s, const double2* grids, int nl, int nx, int ny, const ModeDims& d,
+               int axis_y, double2* out, void* scratch, int* bad);
+size_t li_convmat_scratch_bytes(int nl, int nx, int ny, const ModeDims& d);
 
 // Per-source wave vectors (rcwa.cpp:85-160) and gap modes (rcwa.cpp:163-234).
 // One solve's source plus its lattice periods: a sweep repeats the stack's
@@ -92,10 +98,12 @@ int wave_vectors(cudaStream_t s, const SourceDev* src_dev, int B, const ModeDims
                  const WaveVecs& w, uint32_t* status);
 
 // P and Q of a patterned layer (rcwa.cpp:262-286) from erc^-1 / urc^-1.
+// exx/eyy multiply E_x/E_y in Q, mxx/myy multiply H_x/H_y in P: erc, erc,
+// urc, urc under the reference's Laurent rule, Li's matrices otherwise.
 // Item b reads its matrices at offset b * s_item (0: one set for all items).
-int assemble_pq(cudaStream_t s, int B, const ModeDims& d, const double2* erc, const double2* urc,
-                const double2* einv, const double2* uinv, long long s_item, const WaveVecs& w,
-                double2* P, double2* Qm);
+int assemble_pq(cudaStream_t s, int B, const ModeDims& d, const double2* exx, const double2* eyy,
+                const double2* mxx, const double2* myy, const double2* einv, const double2* uinv,
+                long long s_item, const WaveVecs& w, double2* P, double2* Qm);
 // lam = usqrt(lam2), ilam = 1/lam, X = exp(-k0 t lam) (rcwa.cpp:317, 329, 339).
 // t_item (device, may be null): item b's thickness at t_item[b * t_stride].
 int layer_modes(cudaStream_t s, int B, int n, const double2* lam2, const double2* kinc,

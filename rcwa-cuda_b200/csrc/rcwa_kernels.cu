@@ -130,6 +130,121 @@ __global__ void convmat_gather_kernel(const double2* __restrict__ Cg, int P, int
 }
 
 // ---------------------------------------------------------------------------
+// Li's factorization rule (L. Li, J. Opt. Soc. Am. A 14, 2758 (1997)), an
+// option beside the reference's Laurent rule: eps_aa = [[ [[eps]]_a ]]_b.
+// Along every grid line of axis a (fixed coordinate ib on the other axis b)
+// the Pa x Pa Toeplitz matrix of 1/eps is formed and inverted; the inverses
+// are then convolved along b and gathered into the N x N mode matrix
+// (m = p*Q + q).  Axis a = x: lines are grid rows (stride 1); a = y: grid
+// columns (stride nx).  The DFT coefficients follow the ConvMat conventions
+// above: 1/n normalisation and 0 where k + n/2 falls outside [0, n).
+// ---------------------------------------------------------------------------
+
+// One CTA per (line ib, layer l): the line's reciprocals and the twiddles in
+// shared memory, one warp per coefficient k = u - (Pa-1), then the augmented
+// system [T | I] (Pa x 2Pa, column-major) with T(p, p') = a(p - p').
+__global__ void __launch_bounds__(256)
+li_line_kernel(const double2* __restrict__ grids, int na, int nb, long long sa, long long sb,
+               long long sl, int Pa, const double2* __restrict__ tw_a, double2* __restrict__ aug,
+               int* __restrict__ bad) {
+  extern __shared__ __align__(16) double2 sm[];
+  double2* line = sm;          // [na]
+  double2* tw = sm + na;       // [na]
+  double2* coef = tw + na;     // [2Pa-1]
+  const int ib = blockIdx.x, l = blockIdx.y;
+  const double2* src = grids + l * sl + ib * sb;
+  bool nonfinite = false;
+  for (int i = threadIdx.x; i < na; i += blockDim.x) {
+    const double2 r = crcp(src[i * sa]);
+    nonfinite |= !(isfinite(r.x) && isfinite(r.y));
+    line[i] = r;
+    tw[i] = tw_a[i];
+  }
+  if (__syncthreads_or(nonfinite) && threadIdx.x == 0) atomicOr(bad, 1);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int nu = 2 * Pa - 1;
+  for (int u = wid; u < nu; u += nw) {
+    const int k = u - (Pa - 1);
+    double sr = 0.0, si = 0.0;
+    if (k + na / 2 >= 0 && k + na / 2 < na) {
+      const int km = ((k % na) + na) % na;
+      int idx = (int)(((long long)km * lane) % na);
+      const int step = (int)(((long long)km * 32) % na);
+      for (int i = lane; i < na; i += 32) {
+        const double2 f = line[i], w = tw[idx];
+        sr = fma(f.x, w.x, fma(-f.y, w.y, sr));
+        si = fma(f.x, w.y, fma(f.y, w.x, si));
+        idx += step;
+        if (idx >= na) idx -= na;
+      }
+      sr = warp_sum(sr) / (double)na;
+      si = warp_sum(si) / (double)na;
+    }
+    if (lane == 0) coef[u] = cmk(sr, si);
+  }
+  __syncthreads();
+  double2* A = aug + ((long long)l * nb + ib) * 2 * Pa * Pa;
+  for (int e = threadIdx.x; e < 2 * Pa * Pa; e += blockDim.x) {
+    const int r = e % Pa, c = e / Pa;
+    A[e] = c < Pa ? coef[r - c + Pa - 1] : cmk(r == c - Pa ? 1.0 : 0.0, 0.0);
+  }
+}
+
+// Laurent pass along b: Cg[l][v][p'][p] = (1/nb) sum_ib M_ib(p, p') w_nb^(kb ib),
+// kb = v - (Pb-1), M_ib the inverse in the right half of line ib's system.
+// One warp per (p, p', v).
+__global__ void __launch_bounds__(256)
+li_cross_kernel(const double2* __restrict__ aug, int nb, int Pa, int Pb,
+                const double2* __restrict__ tw_b, double2* __restrict__ Cg) {
+  const int l = blockIdx.y;
+  const int nv = 2 * Pb - 1, PP = Pa * Pa;
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (gw >= PP * nv) return;
+  const int e = gw % PP, v = gw / PP;      // e = p' * Pa + p (column-major element)
+  const int kb = v - (Pb - 1);
+  double2 out = cmk(0.0, 0.0);
+  if (kb + nb / 2 >= 0 && kb + nb / 2 < nb) {
+    const int km = ((kb % nb) + nb) % nb;
+    int idx = (int)(((long long)km * lane) % nb);
+    const int step = (int)(((long long)km * 32) % nb);
+    double sr = 0.0, si = 0.0;
+    const double2* M = aug + (long long)l * nb * 2 * PP + PP + e;
+    for (int ib = lane; ib < nb; ib += 32) {
+      const double2 f = M[(long long)ib * 2 * PP], w = tw_b[idx];
+      sr = fma(f.x, w.x, fma(-f.y, w.y, sr));
+      si = fma(f.x, w.y, fma(f.y, w.x, si));
+      idx += step;
+      if (idx >= nb) idx -= nb;
+    }
+    out = cmk(warp_sum(sr) / (double)nb, warp_sum(si) / (double)nb);
+  }
+  if (lane == 0) Cg[((long long)l * nv + v) * PP + e] = out;
+}
+
+// bad |= 2 when any line's Toeplitz system reported a zero pivot
+__global__ void li_any_kernel(const uint32_t* __restrict__ st, long long n, int* bad) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (__syncthreads_or(i < n && st[i] != 0) && threadIdx.x == 0) atomicOr(bad, 2);
+}
+
+// out(m, n) = Cg[v = b_m - b_n + Pb - 1][a_n][a_m], (a, b) = (p, q) for axis
+// x and (q, p) for axis y.
+__global__ void li_gather_kernel(const double2* __restrict__ Cg, int P, int Q, int axis_y,
+                                 double2* __restrict__ out) {
+  const int N = P * Q;
+  const int l = blockIdx.y;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)N * N) return;
+  const int m = (int)(e % N), n = (int)(e / N);
+  const int Pa = axis_y ? Q : P, Pb = axis_y ? P : Q;
+  const int am = axis_y ? m % Q : m / Q, bm = axis_y ? m / Q : m % Q;
+  const int an = axis_y ? n % Q : n / Q, bn = axis_y ? n / Q : n % Q;
+  const long long PP = (long long)Pa * Pa;
+  out[(long long)l * N * N + e] = Cg[((long long)l * (2 * Pb - 1) + (bm - bn + Pb - 1)) * PP + an * Pa + am];
+}
+
+// ---------------------------------------------------------------------------
 // K2: wave vectors (rcwa.cpp:85-160) and gap modes (rcwa.cpp:163-234).
 // ---------------------------------------------------------------------------
 __global__ void wavevec_kernel(const SourceDev* __restrict__ srcs, int nxh,
@@ -185,10 +300,14 @@ __global__ void wavevec_kernel(const SourceDev* __restrict__ srcs, int nxh,
 
 // ---------------------------------------------------------------------------
 // P_i and Q_i of a patterned layer (rcwa.cpp:262-286); Kx/Ky diagonal, so
-// erc^-1 diag(K) is a column scaling of erc^-1.
+// erc^-1 diag(K) is a column scaling of erc^-1.  exx/eyy/mxx/myy are the
+// in-plane permittivity / permeability matrices (all erc / urc under the
+// reference's Laurent rule).
 // ---------------------------------------------------------------------------
-__global__ void assemble_pq_kernel(int N, const double2* __restrict__ erc,
-                                   const double2* __restrict__ urc,
+__global__ void assemble_pq_kernel(int N, const double2* __restrict__ exx,
+                                   const double2* __restrict__ eyy,
+                                   const double2* __restrict__ mxx,
+                                   const double2* __restrict__ myy,
                                    const double2* __restrict__ einv,
                                    const double2* __restrict__ uinv, long long s_item,
                                    const double2* __restrict__ Kxg,
@@ -204,17 +323,17 @@ __global__ void assemble_pq_kernel(int N, const double2* __restrict__ erc,
   const double2* Kx = Kxg + (long long)b * N;
   const double2* Ky = Kyg + (long long)b * N;
   const long long o = (long long)b * s_item + (long long)jj * N + ii;
-  const double2 ei = einv[o], ui = uinv[o], ec = erc[o], uc = urc[o];
+  const double2 ei = einv[o], ui = uinv[o];
   double2 p, q;
   if (!bi && !bj) {
     p = cmul(Kx[ii], cmul(ei, Ky[jj]));                   // :273
     q = cmul(Kx[ii], cmul(ui, Ky[jj]));                   // :282
   } else if (!bi && bj) {
-    p = csub(uc, cmul(Kx[ii], cmul(ei, Kx[jj])));         // :274
-    q = csub(ec, cmul(Kx[ii], cmul(ui, Kx[jj])));         // :283
+    p = csub(myy[o], cmul(Kx[ii], cmul(ei, Kx[jj])));     // :274
+    q = csub(eyy[o], cmul(Kx[ii], cmul(ui, Kx[jj])));     // :283
   } else if (bi && !bj) {
-    p = csub(cmul(Ky[ii], cmul(ei, Ky[jj])), uc);         // :275
-    q = csub(cmul(Ky[ii], cmul(ui, Ky[jj])), ec);         // :284
+    p = csub(cmul(Ky[ii], cmul(ei, Ky[jj])), mxx[o]);     // :275
+    q = csub(cmul(Ky[ii], cmul(ui, Ky[jj])), exx[o]);     // :284
   } else {
     p = cmul(cneg(Ky[ii]), cmul(ei, Kx[jj]));             // :276
     q = cmul(cneg(Ky[ii]), cmul(ui, Kx[jj]));             // :285
@@ -676,6 +795,70 @@ int convmat(cudaStream_t s, const double2* grids, int nl, int nx, int ny, const 
   return RCWA_OK;
 }
 
+static size_t li_axis_bytes(int nl, int na, int nb, int Pa, int Pb) {
+  const size_t PP = (size_t)Pa * Pa, lines = (size_t)nl * nb;
+  return ((size_t)na + nb + lines * 2 * PP + (size_t)nl * (2 * Pb - 1) * PP) * sizeof(double2) +
+         lines * (Pa * sizeof(int) + sizeof(uint32_t)) + 1024;
+}
+
+size_t li_convmat_scratch_bytes(int nl, int nx, int ny, const ModeDims& d) {
+  const size_t a = li_axis_bytes(nl, nx, ny, d.P, d.Q), b = li_axis_bytes(nl, ny, nx, d.Q, d.P);
+  return a > b ? a : b;
+}
+
+int li_convmat(cudaStream_t s, const double2* grids, int nl, int nx, int ny, const ModeDims& d,
+               int axis_y, double2* out, void* scratch, int* bad) {
+  if (nl <= 0) return RCWA_OK;
+  const int na = axis_y ? ny : nx, nb = axis_y ? nx : ny;
+  const int Pa = axis_y ? d.Q : d.P, Pb = axis_y ? d.P : d.Q;
+  const long long sa = axis_y ? nx : 1, sb = axis_y ? 1 : nx, sl = (long long)nx * ny;
+  const size_t PP = (size_t)Pa * Pa, lines = (size_t)nl * nb;
+  double2* tw_a = (double2*)scratch;
+  double2* tw_b = tw_a + na;
+  double2* aug = tw_b + nb;
+  double2* Cg = aug + lines * 2 * PP;
+  int* piv = (int*)(Cg + (size_t)nl * (2 * Pb - 1) * PP);
+  uint32_t* st = (uint32_t*)(piv + lines * Pa);
+  twiddle_kernel<<<cdiv_up(na, 256), 256, 0, s>>>(tw_a, na);
+  count_launch();
+  twiddle_kernel<<<cdiv_up(nb, 256), 256, 0, s>>>(tw_b, nb);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  const size_t shm = ((size_t)2 * na + 2 * Pa - 1) * sizeof(double2);
+  if (shm > 200 * 1024) {
+    set_last_error("Li rule: %d grid points along a line is too many", na);
+    return RCWA_ERR_INVALID;
+  }
+  if (shm > 48 * 1024) {
+    static bool set[64] = {};   // the attribute is per device
+    int dev = 0;
+    RCWA_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64 || !set[dev]) {
+      RCWA_CUDA_TRY(cudaFuncSetAttribute(li_line_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024));
+      if (dev < 64) set[dev] = true;
+    }
+  }
+  li_line_kernel<<<dim3(nb, nl), 256, shm, s>>>(grids, na, nb, sa, sb, sl, Pa, tw_a, aug, bad);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, lines * sizeof(uint32_t), s));
+  int rc = zgesv(s, Pa, Pa, aug, Pa, 2 * (long long)PP, (int)lines, piv, st);
+  if (rc) return rc;
+  li_any_kernel<<<cdiv_up((long long)lines, 256), 256, 0, s>>>(st, (long long)lines, bad);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  const long long warps = (long long)PP * (2 * Pb - 1);
+  li_cross_kernel<<<dim3(cdiv_up(warps, 8), nl), 256, 0, s>>>(aug, nb, Pa, Pb, tw_b, Cg);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  const long long NN = (long long)d.N * d.N;
+  li_gather_kernel<<<dim3(cdiv_up(NN, 256), nl), 256, 0, s>>>(Cg, d.P, d.Q, axis_y, out);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  return RCWA_OK;
+}
+
 int wave_vectors(cudaStream_t s, const SourceDev* src_dev, int B, const ModeDims& d,
                  double2 er_ref, double2 ur_ref, double2 er_trn, double2 ur_trn,
                  const WaveVecs& w, uint32_t* status) {
@@ -686,12 +869,12 @@ int wave_vectors(cudaStream_t s, const SourceDev* src_dev, int B, const ModeDims
   return RCWA_OK;
 }
 
-int assemble_pq(cudaStream_t s, int B, const ModeDims& d, const double2* erc, const double2* urc,
-                const double2* einv, const double2* uinv, long long s_item, const WaveVecs& w,
-                double2* P, double2* Qm) {
+int assemble_pq(cudaStream_t s, int B, const ModeDims& d, const double2* exx, const double2* eyy,
+                const double2* mxx, const double2* myy, const double2* einv, const double2* uinv,
+                long long s_item, const WaveVecs& w, double2* P, double2* Qm) {
   const long long nn = (long long)d.n * d.n;
-  assemble_pq_kernel<<<dim3(cdiv_up(nn, 256), B), 256, 0, s>>>(d.N, erc, urc, einv, uinv, s_item,
-                                                                w.Kx, w.Ky, P, Qm);
+  assemble_pq_kernel<<<dim3(cdiv_up(nn, 256), B), 256, 0, s>>>(d.N, exx, eyy, mxx, myy, einv, uinv,
+                                                                s_item, w.Kx, w.Ky, P, Qm);
   count_launch();
   RCWA_LAUNCH_CHECK();
   return RCWA_OK;

@@ -75,11 +75,12 @@ void geometry_free(rcwa_geometry* g) {
   if (g->urc) cudaFreeAsync(g->urc, s);
   if (g->einv) cudaFreeAsync(g->einv, s);
   if (g->uinv) cudaFreeAsync(g->uinv, s);
-  g->erc = g->urc = g->einv = g->uinv = nullptr;
+  if (g->li) cudaFreeAsync(g->li, s);
+  g->erc = g->urc = g->einv = g->uinv = g->li = nullptr;
 }
 
 int geometry_build(rcwa_context* ctx, rcwa_geometry* g, const rcwa_stack* st,
-                   const rcwa_params* p, int on_device) {
+                   const rcwa_params* p, int on_device, unsigned opts) {
   cudaStream_t s = ctx->stream;
   const ModeDims d = dims_of(p);
   g->ctx = ctx;
@@ -198,6 +199,32 @@ int geometry_build(rcwa_context* ctx, rcwa_geometry* g, const rcwa_stack* st,
                                     cudaMemcpyDeviceToDevice, s));
       RCWA_CUDA_TRY(cudaMemcpyAsync(g->uinv + pat[k] * NN, aug + (np + k) * s2 + NN,
                                     NN * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  if ((opts & RCWA_GEOM_LI_RULE) && np > 0) {
+    // eps_xx, eps_yy, mu_xx, mu_yy of every layer (uniform layers never read them)
+    const size_t m = (size_t)nl * NN;
+    RCWA_CUDA_TRY(cudaMallocAsync((void**)&g->li, 4 * m * sizeof(double2), s));
+    char* lscr = nullptr;
+    const size_t lb = li_convmat_scratch_bytes(nl, st->nx, st->ny, d);
+    RCWA_CUDA_TRY(cudaMallocAsync((void**)&lscr, lb + 256, s));
+    int* bad = (int*)(lscr + lb);
+    cudaError_t e = cudaMemsetAsync(bad, 0, sizeof(int), s);
+    for (int k = 0; k < 4 && !rc && e == cudaSuccess; ++k)
+      rc = li_convmat(s, k < 2 ? der : dur, nl, st->nx, st->ny, d, k & 1, g->li + k * m, lscr, bad);
+    int hbad = 0;
+    if (!rc && e == cudaSuccess) e = cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFreeAsync(lscr, s);
+    if (rc) return rc;
+    if (e != cudaSuccess) {
+      set_last_error("Li rule: %s", cudaGetErrorString(e));
+      return RCWA_ERR_CUDA;
+    }
+    if (hbad) {
+      set_last_error(hbad & 1 ? "Li rule: a layer grid holds a zero or non-finite permittivity / permeability"
+                              : "Li rule: singular Toeplitz matrix of 1/eps along a grid line");
+      return RCWA_ERR_NUMERIC;
     }
   }
   RCWA_CUDA_TRY(cudaStreamSynchronize(s));
@@ -385,6 +412,17 @@ int fold_status(cudaStream_t s, uint32_t* dst, const uint32_t* scratch, int B, i
 
 // S-matrix of one patterned layer (rcwa.cpp:254-352) for the chunk.
 // Output: S11 at augD[1] (stride 3n^2) and S12 in s2.
+// P -> pl.s0, Q -> pl.s1 of patterned layer l (rcwa.cpp:262-286) for B items.
+static int layer_pq(cudaStream_t s, const Layers& g, int l, int B, Plan& pl) {
+  const long long lo = l * g.s_layer;
+  const double2* exx = g.exx ? g.exx + lo : g.erc + lo;
+  const double2* eyy = g.eyy ? g.eyy + lo : g.erc + lo;
+  const double2* mxx = g.mxx ? g.mxx + lo : g.urc + lo;
+  const double2* myy = g.myy ? g.myy + lo : g.urc + lo;
+  return assemble_pq(s, B, g.d, exx, eyy, mxx, myy, g.einv + lo, g.uinv + lo, g.s_item, pl.wv,
+                     pl.s0, pl.s1);
+}
+
 // Omega^2 = P Q of patterned layer l (rcwa.cpp:262-288) for the chunk -> out
 // (packed n x n per source).
 int layer_omega2(rcwa_context* ctx, const Layers& g, int l, Plan& pl, double2* out) {
@@ -393,10 +431,7 @@ int layer_omega2(rcwa_context* ctx, const Layers& g, int l, Plan& pl, double2* o
   const int B = pl.B, n = d.n;
   const long long nn = (long long)n * n;
   int rc;
-  const long long lo = l * g.s_layer;
-  if ((rc = assemble_pq(s, B, d, g.erc + lo, g.urc + lo, g.einv + lo, g.uinv + lo, g.s_item, pl.wv,
-                        pl.s0, pl.s1)))
-    return rc;
+  if ((rc = layer_pq(s, g, l, B, pl))) return rc;
   ZGemm gm;
   gm.m = n; gm.n = n; gm.k = n; gm.batch = B;
   gm.A = pl.s0; gm.lda = n; gm.sA = nn;
@@ -457,10 +492,7 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
   int rc;
   // Q_i (:280-286) again (P is not needed past Omega^2)
-  const long long lo = l * g.s_layer;
-  if ((rc = assemble_pq(s, B, d, g.erc + lo, g.urc + lo, g.einv + lo, g.uinv + lo, g.s_item, pl.wv,
-                        pl.s0, pl.s1)))
-    return rc;
+  if ((rc = layer_pq(s, g, l, B, pl))) return rc;
   // W into the first half of [W | I]
   if ((rc = copy_blocks(s, pl.augWV, s2, Wl, nn, nn, B))) return rc;
   ZGemm gm;
@@ -680,6 +712,13 @@ Layers layers_of(const rcwa_geometry* g) {
   G.einv = g->einv;
   G.uinv = g->uinv;
   G.s_layer = (long long)g->d.N * g->d.N;
+  if (g->li) {
+    const long long m = (long long)g->nl * G.s_layer;
+    G.exx = g->li;
+    G.eyy = g->li + m;
+    G.mxx = g->li + 2 * m;
+    G.myy = g->li + 3 * m;
+  }
   G.s_item = 0;
   return G;
 }

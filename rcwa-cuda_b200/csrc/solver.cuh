@@ -42,6 +42,9 @@ struct rcwa_geometry {
   double2* urc = nullptr;
   double2* einv = nullptr;  // [nl][N*N], patterned layers only
   double2* uinv = nullptr;
+  // Li's factorization rule (RCWA_GEOM_LI_RULE): [4][nl][N*N] eps_xx, eps_yy,
+  // mu_xx, mu_yy; null under the reference's Laurent rule
+  double2* li = nullptr;
 };
 
 namespace rcwa {
@@ -63,6 +66,8 @@ struct Layers {
   const double2* ueps = nullptr;   // host [nl], shared
   const double2* umu = nullptr;
   const double2 *erc = nullptr, *urc = nullptr, *einv = nullptr, *uinv = nullptr;
+  // in-plane matrices of Li's rule (same layout as erc); null: erc / urc
+  const double2 *exx = nullptr, *eyy = nullptr, *mxx = nullptr, *myy = nullptr;
   long long s_layer = 0, s_item = 0;
   const double* t_item = nullptr;
   const double2* ueps_item = nullptr;
@@ -102,7 +107,7 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
 // Build convolution matrices and their inverses.  grids_er/ur are device
 // pointers ([nl][ny][nx]) when on_device, host pointers otherwise.
 int geometry_build(rcwa_context* ctx, rcwa_geometry* g, const rcwa_stack* st,
-                   const rcwa_params* p, int on_device);
+                   const rcwa_params* p, int on_device, unsigned opts = 0);
 void geometry_free(rcwa_geometry* g);
 
 // Sweep over sources (host array) on a prepared geometry; outputs on device.

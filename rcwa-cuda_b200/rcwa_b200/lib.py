@@ -32,6 +32,7 @@ STATUS_WOOD_ANOMALY = 8
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+GEOM_LI_RULE = 1   # rcwa_geometry_create_ex: Li's factorization rule
 
 
 class RcwaError(RuntimeError):
@@ -97,6 +98,8 @@ _SIGS = {
     "rcwa_solve_sweep": ([_VP, C.POINTER(CStack), C.POINTER(CSource), C.c_int, C.POINTER(CParams),
                           C.c_int, C.POINTER(CResult)], C.c_int),
     "rcwa_geometry_create": ([_VP, C.POINTER(CStack), C.POINTER(CParams), C.c_int, C.POINTER(_VP)], C.c_int),
+    "rcwa_geometry_create_ex": ([_VP, C.POINTER(CStack), C.POINTER(CParams), C.c_int, C.c_uint,
+                                 C.POINTER(_VP)], C.c_int),
     "rcwa_geometry_destroy": ([_VP], C.c_int),
     "rcwa_solve_sweep_device": ([_VP, _VP, C.POINTER(CSource), C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_convmat": ([_VP, _VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _VP], C.c_int),
@@ -265,10 +268,16 @@ class Context:
         T = T.reshape(ns, P, Q).transpose(0, 2, 1)
         return R, T, Rt, Tt, stat
 
-    def geometry_create(self, st: StackSpec, p: ParamSpec, er_ptr=None, ur_ptr=None, t_ptr=None):
-        """``rcwa_geometry_create``.  With device pointers (e.g. torch tensors'
+    def geometry_create(self, st: StackSpec, p: ParamSpec, er_ptr=None, ur_ptr=None, t_ptr=None,
+                        rule: str = "laurent"):
+        """``rcwa_geometry_create_ex``.  With device pointers (e.g. torch tensors'
         data_ptr()) the grids are read in place on the GPU; otherwise the
-        host arrays of ``st`` are used."""
+        host arrays of ``st`` are used.  ``rule="li"`` selects Li's
+        factorization rule (RCWA_GEOM_LI_RULE) instead of the reference's
+        Laurent rule."""
+        if rule not in ("laurent", "li"):
+            raise ValueError(f"unknown factorization rule {rule!r}")
+        flags = GEOM_LI_RULE if rule == "li" else 0
         on_dev = er_ptr is not None
         if on_dev:
             cst = CStack(st.Nx, st.Ny, st.num_layers, st.Lx, st.Ly, er_ptr, ur_ptr, t_ptr)
@@ -280,7 +289,8 @@ class Context:
             cst = CStack(st.Nx, st.Ny, st.num_layers, st.Lx, st.Ly, _ptr(er), _ptr(ur), _ptr(t))
         prm = c_params(p)
         h = C.c_void_p()
-        _check(self.lib.rcwa_geometry_create(self.h, C.byref(cst), C.byref(prm), 1 if on_dev else 0, C.byref(h)))
+        _check(self.lib.rcwa_geometry_create_ex(self.h, C.byref(cst), C.byref(prm), 1 if on_dev else 0, flags,
+                                                C.byref(h)))
         del keep
         return h
 
