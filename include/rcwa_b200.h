@@ -283,9 +283,16 @@ int rcwa_eig_noalloc(int n, int batch, const rcwa_complex* A_dev, rcwa_complex* 
 /* PartialPivLU solve (the .lu().solve calls of rcwa.cpp): X = A^-1 B, batched. */
 int rcwa_lu_solve(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_complex* A,
                   const rcwa_complex* B, rcwa_complex* X, uint32_t* status);
-/* C = A * B (n x k times k x m), batched; precision selects FP64 or split-TF32. */
+/* C = A * B (m x k times k x n, column-major host arrays), batched; precision
+ * selects FP64 or split-TF32 (the Eigen operator* products of rcwa.cpp). */
 int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_complex* A,
               const rcwa_complex* B, rcwa_complex* C, int precision);
+/* C = alpha op(A) op(B) + beta C, batched, column-major host arrays; op = 1
+ * takes the conjugate transpose (A stored k x m, B stored n x k), C is read
+ * when beta != 0.  FP64 only. */
+int rcwa_gemm_ex(rcwa_context* ctx, int opa, int opb, int m, int n, int k, int batch,
+                 rcwa_complex alpha, const rcwa_complex* A, const rcwa_complex* B, rcwa_complex beta,
+                 rcwa_complex* C);
 
 #ifdef __cplusplus
 }

@@ -528,4 +528,33 @@ int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_comp
   return RCWA_OK;
 }
 
+int rcwa_gemm_ex(rcwa_context* ctx, int opa, int opb, int m, int n, int k, int batch,
+                 rcwa_complex alpha, const rcwa_complex* A, const rcwa_complex* B, rcwa_complex beta,
+                 rcwa_complex* C) {
+  CHECK_ARG(ctx && A && B && C && m > 0 && n > 0 && k > 0 && batch > 0, "bad argument");
+  CHECK_ARG((opa == 0 || opa == 1) && (opb == 0 || opb == 1), "op must be 0 or 1");
+  RCWA_CUDA_TRY(cudaSetDevice(ctx->device));
+  const size_t na = (size_t)m * k, nb = (size_t)k * n, nc = (size_t)m * n;
+  int rc = ctx_reserve(ctx, (na + nb + nc) * batch * 16 + 1024);
+  if (rc) return rc;
+  double2* dA = (double2*)ctx->ws;
+  double2* dB = dA + na * batch;
+  double2* dC = dB + nb * batch;
+  cudaStream_t s = ctx->stream;
+  RCWA_CUDA_TRY(cudaMemcpyAsync(dA, A, na * batch * 16, cudaMemcpyHostToDevice, s));
+  RCWA_CUDA_TRY(cudaMemcpyAsync(dB, B, nb * batch * 16, cudaMemcpyHostToDevice, s));
+  RCWA_CUDA_TRY(cudaMemcpyAsync(dC, C, nc * batch * 16, cudaMemcpyHostToDevice, s));
+  ZGemm g;
+  g.m = m; g.n = n; g.k = k; g.batch = batch;
+  g.alpha = make_double2(alpha.re, alpha.im);
+  g.beta = make_double2(beta.re, beta.im);
+  g.A = dA; g.lda = opa ? k : m; g.sA = (long long)na; g.opA = opa;
+  g.B = dB; g.ldb = opb ? n : k; g.sB = (long long)nb; g.opB = opb;
+  g.C = dC; g.ldc = m; g.sC = (long long)nc;
+  if ((rc = zgemm(s, g))) return rc;
+  RCWA_CUDA_TRY(cudaMemcpyAsync(C, dC, nc * batch * 16, cudaMemcpyDeviceToHost, s));
+  RCWA_CUDA_TRY(cudaStreamSynchronize(s));
+  return RCWA_OK;
+}
+
 }  // extern "C"

@@ -155,14 +155,109 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
       : "d"(a), "d"(b));
 }
 
+// Thin strips: when m (or n) is a little above a multiple of the 64-wide
+// tile (n = 450 = 7 * 64 + 2), a last row of 64-wide tiles would hold only a
+// few live rows and still cost nearly a full tile (its loads and pipeline do
+// not shrink).  The DMMA launch then tiles the 64-aligned part and gives the
+// last rows (ROWS = 1, all n columns) and columns (ROWS = 0, the aligned
+// rows), at most 16 of each, to extra CTAs of the same grid, which run this
+// GEMV-like pass alongside the tensor-core tiles.  One call: the output
+// block rows [r0, r1) x cols [c0, c1), at most 64 along the long side and 16
+// along the short one; k staged through shared memory (sm: 16 x 65 + 16 x 17
+// double2) in steps of 16, loads coalesced along whichever index is
+// contiguous in memory; thread t owns long index t % 64 and short indices
+// SPT (t / 64) + {0..SPT-1}.  A, B, C, dl, dr point at this batch item.
+template <int OPA, int OPB, int ROWS, int NTH>
+__device__ __forceinline__ void thin_tile(int r0, int r1, int c0, int c1, int k, double2 alpha,
+                                          const double2* __restrict__ A, int lda,
+                                          const double2* __restrict__ B, int ldb, double2 beta,
+                                          double2* __restrict__ C, int ldc,
+                                          const double2* __restrict__ dl,
+                                          const double2* __restrict__ dr, double2* sm) {
+  constexpr int TK = 16, TL = 64, TS = 16, SPT = TS / (NTH / TL);
+  double2 (*Ls)[TL + 1] = reinterpret_cast<double2 (*)[TL + 1]>(sm);                 // [k][long]
+  double2 (*Ss)[TS + 1] = reinterpret_cast<double2 (*)[TS + 1]>(sm + TK * (TL + 1));  // [k][short]
+  const int nl = ROWS ? c1 - c0 : r1 - r0, ns = ROWS ? r1 - r0 : c1 - c0;
+  const int tid = threadIdx.x, li = tid % TL, sg = tid / TL;
+  // A(i, kk) and B(kk, j) with the operand ops applied, 0 outside the block
+  auto a_at = [&](int i, int kk) -> double2 {
+    if (i >= r1 || kk >= k) return cmk(0.0, 0.0);
+    return OPA ? cconj(A[(long long)i * lda + kk]) : A[(long long)kk * lda + i];
+  };
+  auto b_at = [&](int kk, int j) -> double2 {
+    if (kk >= k || j >= c1) return cmk(0.0, 0.0);
+    return OPB ? cconj(B[(long long)kk * ldb + j]) : B[(long long)j * ldb + kk];
+  };
+  double2 acc[SPT];
+#pragma unroll
+  for (int q = 0; q < SPT; ++q) acc[q] = cmk(0.0, 0.0);
+  for (int k0 = 0; k0 < k; k0 += TK) {
+#pragma unroll
+    for (int h = 0; h < TK * TL / NTH; ++h) {   // long operand, 64 x 16
+      const int e = tid + NTH * h;
+      if (ROWS) {
+        const bool kfast = !OPB;   // B(kk, j) runs along kk in memory unless transposed
+        const int kk = kfast ? e % TK : e / TL, l = kfast ? e / TK : e % TL;
+        Ls[kk][l] = b_at(k0 + kk, c0 + l);
+      } else {
+        const bool kfast = OPA;    // A(i, kk) runs along i in memory unless transposed
+        const int kk = kfast ? e % TK : e / TL, l = kfast ? e / TK : e % TL;
+        Ls[kk][l] = a_at(r0 + l, k0 + kk);
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < TK * TS / NTH; ++h) {   // short operand, 16 x 16
+      const int e = tid + NTH * h;
+      if (ROWS) {
+        const bool kfast = OPA;
+        const int kk = kfast ? e % TK : e / TS, q = kfast ? e / TK : e % TS;
+        Ss[kk][q] = a_at(r0 + q, k0 + kk);
+      } else {
+        const bool kfast = !OPB;
+        const int kk = kfast ? e % TK : e / TS, q = kfast ? e / TK : e % TS;
+        Ss[kk][q] = b_at(k0 + kk, c0 + q);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < TK; ++kk) {
+      const double2 lv = Ls[kk][li];
+#pragma unroll
+      for (int q = 0; q < SPT; ++q) {
+        const double2 sv = Ss[kk][sg * SPT + q];
+        acc[q].x = fma(lv.x, sv.x, fma(-lv.y, sv.y, acc[q].x));
+        acc[q].y = fma(lv.x, sv.y, fma(lv.y, sv.x, acc[q].y));
+      }
+    }
+    __syncthreads();
+  }
+  if (li >= nl) return;
+  const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
+#pragma unroll
+  for (int q = 0; q < SPT; ++q) {
+    const int sidx = sg * SPT + q;
+    if (sidx >= ns) continue;
+    const int row = ROWS ? r0 + sidx : r0 + li, col = ROWS ? c0 + li : c0 + sidx;
+    double2 v = cmul(alpha, acc[q]);
+    if (dl) v = cmul(dl[row], v);
+    if (dr) v = cmul(v, dr[col]);
+    double2* cp = C + (long long)col * ldc + row;
+    if (use_beta) v = cadd(v, cmul(beta, *cp));
+    *cp = v;
+  }
+}
+
 // WM warps along M x 2 along N, each a 32x32 complex tile: CTA tile
-// (32 WM) x 64, 64 WM threads.
+// (32 WM) x 64, 64 WM threads.  The tiles cover rows [0, m) x cols [0, n);
+// with mf > m or nf > n, the first thin_rows rows of the grid are thin-strip
+// CTAs for rows [m, mf) x cols [0, nf) and rows [0, m) x cols [n, nf).
 template <int OPA, int OPB, int WM, int ST>
 __global__ void __launch_bounds__(64 * WM, (WM > 2 ? 1 : 2))
 zgemm_dmma_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, int lda,
                   long long sA, const double2* __restrict__ B, int ldb, long long sB, double2 beta,
                   double2* __restrict__ C, int ldc, long long sC, const double2* __restrict__ dl,
-                  long long sdl, const double2* __restrict__ dr, long long sdr) {
+                  long long sdl, const double2* __restrict__ dr, long long sdr, int mf, int nf,
+                  int thin_rows) {
   constexpr int DT = 64 * WM, TM = 32 * WM;
   // rows padded by two elements: the fragment loads (4 k x 8 rows per
   // quarter-warp pattern) then hit distinct shared-memory banks
@@ -174,7 +269,20 @@ zgemm_dmma_kernel(int m, int n, int k, double2 alpha, const double2* __restrict_
   A += (long long)b * sA;
   B += (long long)b * sB;
   C += (long long)b * sC;
-  const int m0 = blockIdx.y * TM, n0 = blockIdx.x * BN;
+  if ((int)blockIdx.y < thin_rows) {   // thin-strip CTA (the whole CTA takes this branch)
+    const int t = blockIdx.y * gridDim.x + blockIdx.x;
+    const int nrow = mf > m ? (nf + 63) / 64 : 0, ncol = nf > n ? (m + 63) / 64 : 0;
+    const double2* dlb = dl ? dl + (long long)b * sdl : nullptr;
+    const double2* drb = dr ? dr + (long long)b * sdr : nullptr;
+    if (t < nrow)
+      thin_tile<OPA, OPB, 1, DT>(m, mf, t * 64, min(nf, t * 64 + 64), k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                 dlb, drb, dsm);
+    else if (t < nrow + ncol)
+      thin_tile<OPA, OPB, 0, DT>((t - nrow) * 64, min(m, (t - nrow) * 64 + 64), n, nf, k, alpha, A, lda, B,
+                                 ldb, beta, C, ldc, dlb, drb, dsm);
+    return;
+  }
+  const int m0 = (blockIdx.y - thin_rows) * TM, n0 = blockIdx.x * BN;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp % WM, wn = warp / WM;
   const int lr = lane >> 2, lk = lane & 3;
@@ -287,6 +395,19 @@ zgemm_dmma_kernel(int m, int n, int k, double2 alpha, const double2* __restrict_
     }
 }
 
+// Rows / columns past the last multiple of 64 that go to thin-strip CTAs
+// (0: the tensor-core tiles cover them).  RCWA_ZGEMM_THIN=0 (read once)
+// keeps whole 64-wide tiles everywhere.
+int thin_cut(int extent) {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = getenv("RCWA_ZGEMM_THIN");
+    on = (e && strcmp(e, "0") == 0) ? 0 : 1;
+  }
+  const int r = extent % 64;
+  return (on && extent > 64 && r != 0 && r <= 16) ? r : 0;
+}
+
 // Kernel choice.  Default: the DMMA kernel for k > 64 and the CUDA-core
 // kernel for the rank-k updates (k <= 64) of the LU factorisations -- in the
 // C2 sweep on B200 the DMMA kernel ran the k = 450 GEMMs at 21.8 TFLOP/s
@@ -303,7 +424,7 @@ int gemm_impl(int k) {
 }
 
 template <int WM, int ST>
-int launch_dmma(cudaStream_t s, const ZGemm& g, dim3 grid) {
+int launch_dmma(cudaStream_t s, const ZGemm& g, dim3 grid, int cm = 0, int cn = 0) {
   constexpr int smem = ST * BK * (32 * WM + 2 + BN + 2) * (int)sizeof(double2);
   static bool attr[64] = {};   // per device
   int dev = 0;
@@ -315,11 +436,17 @@ int launch_dmma(cudaStream_t s, const ZGemm& g, dim3 grid) {
     RCWA_CUDA_TRY(cudaFuncSetAttribute(zgemm_dmma_kernel<1, 1, WM, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     if (dev < 64) attr[dev] = true;
   }
-  grid.y = cdiv_up(g.m, 32 * WM);
+  // tiles over rows [0, m - cm) x cols [0, n - cn); the thin-strip CTAs
+  // come first in the grid so that they start with the first tiles
+  const int mm = g.m - cm, nm = g.n - cn;
+  grid.x = cdiv_up(nm, BN);
+  const int thin = (cm ? cdiv_up(g.n, 64) : 0) + (cn ? cdiv_up(mm, 64) : 0);
+  const int thin_rows = cdiv_up(thin, (int)grid.x);
+  grid.y = cdiv_up(mm, 32 * WM) + thin_rows;
   const int kk = g.k < 0 ? 0 : g.k;
-#define RCWA_DMMA_ARGS                                                                          \
-  g.m, g.n, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
-      g.dr, g.sdr
+#define RCWA_DMMA_ARGS                                                                           \
+  mm, nm, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
+      g.dr, g.sdr, g.m, g.n, thin_rows
   if (g.opA == 0 && g.opB == 0) zgemm_dmma_kernel<0, 0, WM, ST><<<grid, 64 * WM, smem, s>>>(RCWA_DMMA_ARGS);
   else if (g.opA == 1 && g.opB == 0) zgemm_dmma_kernel<1, 0, WM, ST><<<grid, 64 * WM, smem, s>>>(RCWA_DMMA_ARGS);
   else if (g.opA == 0 && g.opB == 1) zgemm_dmma_kernel<0, 1, WM, ST><<<grid, 64 * WM, smem, s>>>(RCWA_DMMA_ARGS);
@@ -349,7 +476,7 @@ int zgemm(cudaStream_t s, const ZGemm& g) {
   g.m, g.n, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
       g.dr, g.sdr
   if (gemm_impl(kk) == 0) {
-    if ((rc = launch_dmma<2, 4>(s, g, grid))) return rc;
+    if ((rc = launch_dmma<2, 4>(s, g, grid, thin_cut(g.m), thin_cut(g.n)))) return rc;
   } else {
     if (g.opA == 0 && g.opB == 0) zgemm_kernel<0, 0, 4><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
     else if (g.opA == 1 && g.opB == 0) zgemm_kernel<1, 0, 4><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);

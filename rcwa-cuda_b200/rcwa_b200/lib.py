@@ -117,6 +117,8 @@ _SIGS = {
     "rcwa_eig": ([_VP, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_eig_noalloc": ([C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_lu_solve": ([_VP, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
+    "rcwa_gemm_ex": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, CComplex, _VP, _VP,
+                      CComplex, _VP], C.c_int),
     "rcwa_gemm": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, C.c_int], C.c_int),
     "rcwa_rasterize": ([_VP, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.POINTER(CLayerShapes),
                         _VP, _VP, _VP], C.c_int),
@@ -445,6 +447,24 @@ class Context:
         _check(self.lib.rcwa_gemm(self.h, m, n, k, b, _ptr(Af), _ptr(Bf), _ptr(Cf), precision))
         Cm = Cf.transpose(0, 2, 1)
         return Cm[0] if single else Cm
+
+    def gemm_ex(self, A, B, C=None, opa=0, opb=0, alpha=1.0, beta=0.0):
+        """``rcwa_gemm_ex``: alpha op(A) op(B) + beta C on [b, rows, cols]
+        arrays; op = 1 uses the conjugate transpose of the stored matrix."""
+        A = np.asarray(A, dtype=np.complex128)
+        B = np.asarray(B, dtype=np.complex128)
+        b = A.shape[0]
+        m = A.shape[2] if opa else A.shape[1]
+        k = A.shape[1] if opa else A.shape[2]
+        n = B.shape[1] if opb else B.shape[2]
+        Af = np.ascontiguousarray(A.transpose(0, 2, 1))
+        Bf = np.ascontiguousarray(B.transpose(0, 2, 1))
+        Cf = (np.zeros((b, n, m), np.complex128) if C is None
+              else np.ascontiguousarray(np.asarray(C, dtype=np.complex128).transpose(0, 2, 1)))
+        al, be = complex(alpha), complex(beta)
+        _check(self.lib.rcwa_gemm_ex(self.h, opa, opb, m, n, k, b, CComplex(al.real, al.imag), _ptr(Af),
+                                     _ptr(Bf), CComplex(be.real, be.imag), _ptr(Cf)))
+        return Cf.transpose(0, 2, 1)
 
     # ---- device-side rasterisers --------------------------------------------
     @staticmethod

@@ -43,6 +43,24 @@ def test_gemm(ctx, m, n, k, b):
     assert np.abs(Cg - ref).max() <= 1e-13 * math.sqrt(k) * np.abs(ref).max() + 1e-14
 
 
+# sizes just above a multiple of 64 run their last rows / columns through the
+# thin-strip CTAs beside the tensor-core tiles
+@pytest.mark.parametrize("opa,opb", [(0, 0), (1, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("m,n,k,b", [(450, 450, 450, 2), (66, 80, 100, 3), (140, 900, 130, 1),
+                                     (64, 193, 65, 2), (79, 79, 300, 1)])
+def test_gemm_ops_and_thin_edges(ctx, opa, opb, m, n, k, b):
+    rng = np.random.default_rng(m * 3 + n + k + 7 * opa + 11 * opb)
+    A = _rand(rng, b, k, m) if opa else _rand(rng, b, m, k)
+    B = _rand(rng, b, n, k) if opb else _rand(rng, b, k, n)
+    C0 = _rand(rng, b, m, n)
+    alpha, beta = 0.7 - 0.4j, -1.2 + 0.3j
+    Cg = ctx.gemm_ex(A, B, C0, opa, opb, alpha, beta)
+    opA = np.conj(A.transpose(0, 2, 1)) if opa else A
+    opB = np.conj(B.transpose(0, 2, 1)) if opb else B
+    ref = alpha * (opA @ opB) + beta * C0
+    assert np.abs(Cg - ref).max() <= 1e-13 * math.sqrt(k) * np.abs(ref).max() + 1e-14
+
+
 @pytest.mark.parametrize("n,m,b", [(1, 1, 2), (7, 3, 4), (33, 5, 2), (98, 98, 3), (250, 17, 2)])
 def test_lu_solve(ctx, n, m, b):
     rng = np.random.default_rng(n * 7 + m)
