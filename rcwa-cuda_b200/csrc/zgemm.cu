@@ -57,11 +57,25 @@ zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, 
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
 
+  // C += +-A B (alpha = +-1, no diagonal scalings, beta != 0: the LU and
+  // Hessenberg rank-k updates): the accumulators start from +-beta C, read
+  // before the k loop so that the read overlaps the first tile loads instead
+  // of stalling the epilogue; the result is then sgn * acc.
+  const bool pre = !dl && !dr && (beta.x != 0.0 || beta.y != 0.0) && alpha.y == 0.0 &&
+                   (alpha.x == 1.0 || alpha.x == -1.0);
+  const double sgn = pre ? alpha.x : 1.0;
   double2 acc[MI][4];
 #pragma unroll
   for (int i = 0; i < MI; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = cmk(0.0, 0.0);
+    for (int j = 0; j < 4; ++j) {
+      acc[i][j] = cmk(0.0, 0.0);
+      const int row = m0 + tx + 16 * i, col = n0 + ty + 16 * j;
+      if (pre && row < m && col < n) {
+        const double2 c0 = cmul(beta, C[(long long)col * ldc + row]);
+        acc[i][j] = cmk(sgn * c0.x, sgn * c0.y);
+      }
+    }
 
   auto load_tile = [&](int buf, int k0) {
     // A tile: TM rows x 8 k (consecutive threads walk the contiguous index)
@@ -131,10 +145,14 @@ zgemm_kernel(int m, int n, int k, double2 alpha, const double2* __restrict__ A, 
     for (int i = 0; i < MI; ++i) {
       int row = m0 + tx + 16 * i;
       if (row >= m) continue;
+      double2* cp = C + (long long)col * ldc + row;
+      if (pre) {
+        *cp = cmk(sgn * acc[i][j].x, sgn * acc[i][j].y);
+        continue;
+      }
       double2 v = cmul(alpha, acc[i][j]);
       if (dl) v = cmul(dl[(long long)b * sdl + row], v);
       if (dr) v = cmul(v, sr);
-      double2* cp = C + (long long)col * ldc + row;
       if (use_beta) v = cadd(v, cmul(beta, *cp));
       *cp = v;
     }

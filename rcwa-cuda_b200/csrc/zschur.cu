@@ -495,7 +495,7 @@ __device__ void multi_sweep(Smem& sm, double2* stage, double2* H, double2* Z, in
 // reflector, T(0:k, 0:k) is reduced back to Hessenberg form, and V is applied
 // to the rest of H (rows above, columns to the right) and to Z.  The k
 // undeflated eigenvalues serve as the next sweep's shifts.
-constexpr int NWIN = 16;                     // AED window
+constexpr int NWIN = 14;                     // AED window
 constexpr int LDW = NWIN + 1;                // column stride of the window arrays
 constexpr int AED_MIN = NWIN + 16;           // smallest active block that gets AED
 

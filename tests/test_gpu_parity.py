@@ -134,7 +134,7 @@ def test_eig_batched_and_structured(ctx):
 
 def test_eig_aed_paths(ctx):
     """Matrices large enough for aggressive early deflation (active blocks of
-    32 or more): a random one, one with clusters of nearly equal eigenvalues
+    30 or more): a random one, one with clusters of nearly equal eigenvalues
     (many window eigenvalues deflate at once), an exactly degenerate
     diagonalisable one, and an upper-triangular-plus-noise one whose
     eigenvalues are mostly converged on entry."""
