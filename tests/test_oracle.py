@@ -152,3 +152,33 @@ def test_golden_fixtures_reproduce(name):
         r = oracle_solve(pb, i)
         assert np.abs(r.R - z["R"][i]).max() < 1e-12
         assert np.abs(r.T - z["T"][i]).max() < 1e-12
+
+
+@pytest.mark.parametrize("pol", ["TE", "TM"])
+@pytest.mark.parametrize("theta_deg", [0.0, 20.0, 47.0])
+def test_magnetic_uniform_stack_matches_thin_film(pol, theta_deg):
+    """Permeability in the layers and in both half-spaces (rcwa.cpp:361-372,
+    421-432, 579-582) against the characteristic-matrix formulas with mu."""
+    eps = [4.0, 2.2 - 0.3j, 9.5 - 0.05j]
+    mus = [1.7, 2.5 - 0.1j, 1.0]
+    d = [120.0, 75.0, 33.0]
+    st = C.make_stack(700.0, 650.0, [C.uniform(16, 16, e) for e in eps], d,
+                      [C.uniform(16, 16, m) for m in mus])
+    pte, ptm = (1.0, 0.0) if pol == "TE" else (0.0, 1.0)
+    th = math.radians(theta_deg)
+    pb = C.Problem("mu", st, [C.SourceSpec(633.0, th, 0.0, pte, ptm)], C.ParamSpec(2, 2, 1.0, 1.3, 2.25, 1.6))
+    res = oracle_solve(pb)
+    R, T = thin_film_rt(eps, d, 1.0, 2.25, 633.0, th, pol, mus, 1.3, 1.6)
+    assert abs(res.R_tot - R) < 1e-11 and abs(res.T_tot - T) < 1e-11
+
+
+@pytest.mark.parametrize("rule", ["laurent", "li"])
+def test_lossless_magnetic_pattern_conserves_energy(rule):
+    nx, ny, Lx, Ly = 72, 60, 520.0, 470.0
+    er = [C.circle(nx, ny, Lx, Ly, 140.0, 7.5, 1.0), C.lines_x(nx, ny, Lx, 200.0, 3.1, 1.4)]
+    ur = [C.rect(nx, ny, Lx, Ly, 260.0, 150.0, 2.2, 1.0), C.circle(nx, ny, Lx, Ly, 90.0, 1.8, 1.0)]
+    st = C.make_stack(Lx, Ly, er, [110.0, 70.0], ur)
+    pb = C.Problem("m", st, [C.SourceSpec(745.0, 0.35, 0.6, 0.6, 0.8)], C.ParamSpec(3, 2, 1.0, 1.2, 2.25, 1.0))
+    S, src, par = oracle_args(pb, 0)
+    res = O.solve(S, src, par, rule=rule)
+    assert abs(res.R_tot + res.T_tot - 1.0) < 1e-10
