@@ -2,9 +2,8 @@
 bench.py (test infrastructure: the oracle is the checker and the timed CPU
 port, never the product).
 
-The CPU port is timed the way SURVEY's baseline asks for: one solve per
-process with single-threaded BLAS, one process per host core, all cores
-busy.  Worker processes are started with the "spawn" method (the parent has
+The CPU port is timed as one solve per process with single-threaded BLAS,
+one process per host core, all cores busy.  Worker processes are started with the "spawn" method (the parent has
 a CUDA context) and build the wavelength-independent convolution matrices
 once."""
 from __future__ import annotations
