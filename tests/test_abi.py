@@ -47,3 +47,20 @@ def test_last_error_without_gpu(lib):
     assert isinstance(lib.rcwa_last_error(), bytes)
     lib.rcwa_version.restype = ctypes.c_int
     assert lib.rcwa_version() >= 10000
+
+
+def test_cpp_host_api_compiles_and_links(lib, tmp_path):
+    """The C++ host API (reference names on the C ABI) and its demo build
+    against the header and link against the library (nothing is run)."""
+    import shutil
+    import subprocess
+    from rcwa_b200 import build as B
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no g++")
+    demo = os.path.join(ROOT, "rcwa-cuda_b200", "host", "demo_main.cpp")
+    cmd = [gxx, "-std=c++17", "-O1", "-Wall", "-I", os.path.join(ROOT, "include"), demo,
+           "-L", os.path.dirname(B.LIB_PATH), "-lrcwa_b200", "-L/usr/local/cuda/lib64", "-lcudart",
+           "-o", str(tmp_path / "demo")]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
