@@ -45,10 +45,24 @@ extern "C" {
 #define RCWA_STATUS_EIG_NOCONV 2u    /* QR iteration cap hit (rcwa.cpp:300 aborts) */
 #define RCWA_STATUS_NONFINITE 4u     /* non-finite R/T */
 #define RCWA_STATUS_WOOD_ANOMALY 8u  /* some Kz == 0: division at rcwa.cpp:225,541,560 */
+#define RCWA_STATUS_REFINE_SLOW 16u  /* mixed precision: an LU solve's last FP64 refinement
+                                        correction stayed above 1e-4 of |X| */
 
 /* ---- precision modes ---------------------------------------------------- */
 #define RCWA_PREC_FP64 0   /* all-FP64 (parity form, reproduces the reference) */
-#define RCWA_PREC_MIXED 1  /* split-TF32 tensor-core GEMMs + refined FP32 LU; FP64 eig/sqrt/exp/sums */
+#define RCWA_PREC_MIXED 1  /* the stages of rcwa_context_set_mixed (default: all) in reduced
+                              precision; FP64 Omega^2, eig, sqrt, exp and efficiency sums */
+
+/* Stages that RCWA_PREC_MIXED runs in reduced precision.  GEMM stages use the
+ * split-TF32 tensor-core GEMM (each FP64 operand split into TF32 hi + lo,
+ * three tcgen05 kind::tf32 products accumulated in FP32); LU stages factor
+ * and solve in FP32 (complex64) and refine the solution with FP64 residuals
+ * R = B - A X computed on the FP64 tensor cores. */
+#define RCWA_MIXED_LAYER_GEMM 1u  /* V = Q W / lambda and the layer-assembly products (rcwa.cpp:326-348) */
+#define RCWA_MIXED_STAR_GEMM 2u   /* star-product and global-column products (rcwa.cpp:602-611) */
+#define RCWA_MIXED_LAYER_LU 4u    /* W^-1, V^-1, A^-1 and D^-1 solves of a layer (rcwa.cpp:335-348) */
+#define RCWA_MIXED_STAR_LU 8u     /* star-product and global-column solves (rcwa.cpp:605-611) */
+#define RCWA_MIXED_ALL 15u
 
 typedef struct rcwa_complex {
   double re, im;
@@ -119,6 +133,12 @@ int rcwa_context_set_stream(rcwa_context* ctx, void* cuda_stream);
 int rcwa_context_synchronize(rcwa_context* ctx);
 /* Kernels launched by this context since creation (instrumentation). */
 int rcwa_context_kernel_launches(rcwa_context* ctx, uint64_t* count);
+/* Mixed-precision set-up of this context (no reference counterpart: the
+ * reference is FP64 only): the RCWA_MIXED_* stages that RCWA_PREC_MIXED runs
+ * in reduced precision (default RCWA_MIXED_ALL; 0 makes RCWA_PREC_MIXED an
+ * FP64 solve) and the FP64 refinement sweeps of its LU solves (1..4,
+ * default 1).  Sweeps and batches run through the context use it. */
+int rcwa_context_set_mixed(rcwa_context* ctx, unsigned stages, int refine_sweeps);
 
 /* ---- instrumentation (no reference counterpart: the reference only prints
  * to stdout, rcwa.cpp:92-156).  When enabled, the hot kernel families
@@ -269,8 +289,13 @@ int rcwa_eig(rcwa_context* ctx, int n, int batch, const rcwa_complex* A, rcwa_co
  * Scratch lives in one fixed device array of RCWA_EIG_NOALLOC_SCRATCH_BYTES
  * compiled into the library, which every GPU that loads the library holds
  * until the process exits.  Limits: n <= RCWA_EIG_NOALLOC_MAX_N and
- * batch * (3 n^2 + n) * 16 bytes (plus alignment) within the scratch size,
- * otherwise RCWA_ERR_INVALID with the limit in rcwa_last_error().  The first
+ *   bytes(n, batch) = r256(batch n^2 16) + batch (2 n^2 + n) 16
+ *                     + batch (128 n + (ceil(n/32) + 1) 1024) 16 + 256
+ * (input copy; Schur vectors, triangular eigenvectors and reflector scalars;
+ * blocked-Hessenberg panels; r256 rounds up to a multiple of 256) at most
+ * RCWA_EIG_NOALLOC_SCRATCH_BYTES -- the largest batch is 56 at n = 32, 22 at
+ * n = 64, 11 at n = 98 and 7 at n = 128 -- otherwise RCWA_ERR_INVALID with
+ * the bytes needed in rcwa_last_error().  The first
  * call on a device looks up the array's device address once (with that
  * device current); make that first call before any stream capture.  All calls
  * share the one array, which keeps the last call's contents: calls whose GPU
@@ -283,6 +308,12 @@ int rcwa_eig_noalloc(int n, int batch, const rcwa_complex* A_dev, rcwa_complex* 
 /* PartialPivLU solve (the .lu().solve calls of rcwa.cpp): X = A^-1 B, batched. */
 int rcwa_lu_solve(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_complex* A,
                   const rcwa_complex* B, rcwa_complex* X, uint32_t* status);
+/* The same with a precision: RCWA_PREC_FP64 is rcwa_lu_solve; RCWA_PREC_MIXED
+ * factors and solves in FP32 and runs refine_sweeps (1..4) FP64 residual
+ * refinement sweeps (status may carry RCWA_STATUS_REFINE_SLOW). */
+int rcwa_lu_solve_ex(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_complex* A,
+                     const rcwa_complex* B, rcwa_complex* X, uint32_t* status, int precision,
+                     int refine_sweeps);
 /* C = A * B (m x k times k x n, column-major host arrays), batched; precision
  * selects FP64 or split-TF32 (the Eigen operator* products of rcwa.cpp). */
 int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_complex* A,

@@ -329,7 +329,7 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
     rcwa_context* c;
     ~TcScope() { c->tc = 0; }
   } tc_scope{ctx};
-  ctx->tc = precision == RCWA_PREC_MIXED ? 1 : 0;
+  ctx->tc = precision == RCWA_PREC_MIXED ? ctx->mixed_stages : 0u;
   // chunks of every group, sized for a share of the budget each, so that
   // several can run at once
   const int kmax = batch_streams();
@@ -357,7 +357,8 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
     } else {
       for (int l = 0; l < k.nl; ++l) np += k.uniform[l] ? 0 : 1;
     }
-    const size_t per = sweep_bytes_per_source(d, np) + geometry_bytes_per_item(d, nl, k.nx, k.ny);
+    const size_t per = sweep_bytes_per_source(d, np, active_ir_sweeps(ctx)) +
+                       geometry_bytes_per_item(d, nl, k.nx, k.ny);
     int chunk = (int)std::max<size_t>(1, budget / kmax / per);
     // launch grids index matrices in a 65535-wide grid dimension: at most
     // 2 * layers * items systems per batched LU
@@ -406,6 +407,8 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
       th.emplace_back([&, w] {
         rcwa_context* wc = ctx->workers[w];
         wc->tc = ctx->tc;
+        wc->mixed_stages = ctx->mixed_stages;
+        wc->ir_sweeps = ctx->ir_sweeps;
         cudaError_t e = cudaSetDevice(wc->device);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(wc->stream, start, 0);
         cudaGetLastError();   // launch checks below must see only their own launches

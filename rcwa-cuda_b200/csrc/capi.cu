@@ -138,6 +138,15 @@ int rcwa_context_kernel_launches(rcwa_context* c, uint64_t* count) {
   return RCWA_OK;
 }
 
+int rcwa_context_set_mixed(rcwa_context* c, unsigned stages, int refine_sweeps) {
+  CHECK_ARG(c, "NULL context");
+  CHECK_ARG((stages & ~(unsigned)RCWA_MIXED_ALL) == 0, "unknown mixed-precision stage bits");
+  CHECK_ARG(refine_sweeps >= 1 && refine_sweeps <= 4, "refine_sweeps must be 1..4");
+  c->mixed_stages = stages;
+  c->ir_sweeps = refine_sweeps;
+  return RCWA_OK;
+}
+
 int rcwa_geometry_create(rcwa_context* ctx, const rcwa_stack* stack, const rcwa_params* params,
                          int stack_on_device, rcwa_geometry** out) {
   return rcwa_geometry_create_ex(ctx, stack, params, stack_on_device, 0u, out);
@@ -468,20 +477,34 @@ int rcwa_eig(rcwa_context* ctx, int n, int batch, const rcwa_complex* A, rcwa_co
 
 int rcwa_lu_solve(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_complex* A,
                   const rcwa_complex* B, rcwa_complex* X, uint32_t* status) {
+  return rcwa_lu_solve_ex(ctx, n, nrhs, batch, A, B, X, status, RCWA_PREC_FP64, 1);
+}
+
+int rcwa_lu_solve_ex(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_complex* A,
+                     const rcwa_complex* B, rcwa_complex* X, uint32_t* status, int precision,
+                     int refine_sweeps) {
   CHECK_ARG(ctx && A && B && X && n > 0 && nrhs > 0 && batch > 0, "bad argument");
+  CHECK_ARG(precision == RCWA_PREC_FP64 || precision == RCWA_PREC_MIXED, "unknown precision mode");
+  CHECK_ARG(refine_sweeps >= 1 && refine_sweeps <= 4, "refine_sweeps must be 1..4");
   RCWA_CUDA_TRY(cudaSetDevice(ctx->device));
   const size_t nn = (size_t)n * n, nr = (size_t)n * nrhs, sa = nn + nr;
-  const size_t need = sa * batch * 16 + (size_t)n * batch * sizeof(int) + batch * 4 + 1024;
-  int rc = ctx_reserve(ctx, need);
+  const size_t base = ((sa * batch * 16 + (size_t)n * batch * sizeof(int) + batch * 4) + 511) & ~(size_t)255;
+  const size_t irb = precision == RCWA_PREC_MIXED ? zgesv_ir_ws_bytes(n, nrhs, batch, refine_sweeps) : 0;
+  int rc = ctx_reserve(ctx, base + irb + 1024);
   if (rc) return rc;
   double2* dM = (double2*)ctx->ws;
   int* piv = (int*)(dM + sa * batch);
   uint32_t* dst = (uint32_t*)(piv + (size_t)n * batch);
+  void* irws = (char*)ctx->ws + base;
   cudaStream_t s = ctx->stream;
   RCWA_CUDA_TRY(cudaMemcpy2DAsync(dM, sa * 16, A, nn * 16, nn * 16, batch, cudaMemcpyHostToDevice, s));
   RCWA_CUDA_TRY(cudaMemcpy2DAsync(dM + nn, sa * 16, B, nr * 16, nr * 16, batch, cudaMemcpyHostToDevice, s));
   RCWA_CUDA_TRY(cudaMemsetAsync(dst, 0, batch * 4, s));
-  if ((rc = zgesv(s, n, nrhs, dM, n, (long long)sa, batch, piv, dst))) return rc;
+  if (precision == RCWA_PREC_MIXED)
+    rc = zgesv_ir(s, n, nrhs, dM, n, (long long)sa, batch, piv, dst, irws, refine_sweeps);
+  else
+    rc = zgesv(s, n, nrhs, dM, n, (long long)sa, batch, piv, dst);
+  if (rc) return rc;
   RCWA_CUDA_TRY(cudaMemcpy2DAsync(X, nr * 16, dM + nn, sa * 16, nr * 16, batch, cudaMemcpyDeviceToHost, s));
   std::vector<uint32_t> hst(batch);
   RCWA_CUDA_TRY(cudaMemcpyAsync(hst.data(), dst, batch * 4, cudaMemcpyDeviceToHost, s));

@@ -79,6 +79,25 @@ __device__ __forceinline__ double2 cexp(double2 z) {
 }
 __device__ __forceinline__ bool cfinite(double2 a) { return isfinite(a.x) && isfinite(a.y); }
 
+// complex64 (float2) counterparts used by the FP32 factorisation of the
+// mixed-precision LU (zlu.cu)
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ float cabs1(float2 a) { return fabsf(a.x) + fabsf(a.y); }
+__host__ __device__ __forceinline__ float2 cdiv(float2 a, float2 b) {
+  if (fabsf(b.y) <= fabsf(b.x)) {
+    float r = b.y / b.x;
+    float d = b.x + b.y * r;
+    return make_float2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+  } else {
+    float r = b.x / b.y;
+    float d = b.y + b.x * r;
+    return make_float2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+  }
+}
+__host__ __device__ __forceinline__ float2 crcp(float2 b) { return cdiv(make_float2(1.0f, 0.0f), b); }
+
 // ----------------------------------------------------------------------------
 // host-side checking
 // ----------------------------------------------------------------------------

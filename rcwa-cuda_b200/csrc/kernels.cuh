@@ -44,11 +44,16 @@ int zgemm(cudaStream_t s, const ZGemm& g);
 int zgemm_tc(cudaStream_t s, const ZGemm& g, int* err);
 int* tc_error_flag();   // device flag of the current device (set-up once per device)
 
-// X = A^-1 B on the augmented [A | B] (n x (n+nrhs), column-major, ld >= n).
-// tc = 1 runs the trailing and back-substitution updates as split-TF32
-// tensor-core GEMMs (mixed-precision mode).
+// X = A^-1 B on the augmented [A | B] (n x (n+nrhs), column-major, ld >= n),
+// all in FP64; the A part receives the LU factors.
 int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch,
-          int* piv, uint32_t* status, int tc = 0);
+          int* piv, uint32_t* status);
+// The same solve by an FP32 (complex64) LU with `sweeps` FP64 residual
+// refinement sweeps (mixed-precision mode); the A part is left unchanged.
+// ws: zgesv_ir_ws_bytes(n, nrhs, batch, sweeps) bytes of device memory.
+size_t zgesv_ir_ws_bytes(int n, int nrhs, int batch, int sweeps);
+int zgesv_ir(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch,
+             int* piv, uint32_t* status, void* ws, int sweeps);
 
 // Blocked Hessenberg reduction of packed A (zero below the subdiagonal on
 // return) and Z = Q; V is an n x n scratch per matrix, ws hess_ws_bytes().

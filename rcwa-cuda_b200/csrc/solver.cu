@@ -231,6 +231,24 @@ int geometry_build(rcwa_context* ctx, rcwa_geometry* g, const rcwa_stack* st,
   return RCWA_OK;
 }
 
+int active_ir_sweeps(const rcwa_context* ctx) {
+  return (ctx->tc & (RCWA_MIXED_LAYER_LU | RCWA_MIXED_STAR_LU)) ? ctx->ir_sweeps : 0;
+}
+
+// One batched solve of the S-matrix algebra: FP64 LU, or -- when `stage` runs
+// mixed in this solve -- FP32 LU with FP64 refinement in the chunk's
+// refinement workspace.
+static int lu_stage(rcwa_context* ctx, unsigned stage, int n, int nrhs, double2* M, int ld,
+                    long long stride, int batch, int* piv, uint32_t* status) {
+  if (!(ctx->tc & stage)) return zgesv(ctx->stream, n, nrhs, M, ld, stride, batch, piv, status);
+  const size_t need = zgesv_ir_ws_bytes(n, nrhs, batch, ctx->ir_sweeps);
+  if (!ctx->irws || need > ctx->irws_bytes) {
+    set_last_error("internal: refinement workspace of %zu bytes, %zu needed", ctx->irws_bytes, need);
+    return RCWA_ERR_INVALID;
+  }
+  return zgesv_ir(ctx->stream, n, nrhs, M, ld, stride, batch, piv, status, ctx->irws, ctx->ir_sweeps);
+}
+
 // ---------------------------------------------------------------------------
 // Redheffer star product A <- A (x) B (rcwa.cpp:588-615), batched.
 //   augFG holds two stacked batches of n x 3n augmented systems:
@@ -258,7 +276,7 @@ int star_product(rcwa_context* ctx, int B, int n, SMat& A, const SMat& Bm, doubl
     g.B = Y; g.ldb = n; g.sB = sY;
     g.C = C; g.ldc = n; g.sC = sC;
     g.batch = B;
-    g.tc = ctx->tc;
+    g.tc = (ctx->tc & RCWA_MIXED_STAR_GEMM) ? 1 : 0;
     return zgemm(s, g);
   };
   const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
@@ -270,7 +288,7 @@ int star_product(rcwa_context* ctx, int B, int n, SMat& A, const SMat& Bm, doubl
   if ((rc = copy_blocks(s, augG + nn, s3, A.p[2], A.s[2], nn, B))) return rc;
   if ((rc = copy_blocks(s, augG + 2 * nn, s3, A.p[3], A.s[3], nn, B))) return rc;
   // F^-1 [B11 B12], G^-1 [A21 A22] (:605-611), both systems in one batch
-  if ((rc = zgesv(s, n, 2 * n, augFG, n, s3, 2 * B, piv, status, ctx->tc))) return rc;
+  if ((rc = lu_stage(ctx, RCWA_MIXED_STAR_LU, n, 2 * n, augFG, n, s3, 2 * B, piv, status))) return rc;
   // note: status is indexed per system; the caller ORs the two halves.
   const double2* X1 = augF + nn;      // F^-1 B11
   const double2* X2 = augF + 2 * nn;  // F^-1 B12
@@ -331,7 +349,9 @@ struct Plan {
 
 constexpr int kBlocksPerSource = 4 + 1 + 4 + 4 + 2 + 3 + 6;  // SD,tmp,s0-3,augWV,augA,augD,augFG
 
-size_t plan_bytes(const ModeDims& d, int B, int np) {
+// ir > 0: room for the refinement workspace of the largest mixed-precision
+// solve of a chunk (the star product's 2B systems with 2n right-hand sides)
+size_t plan_bytes(const ModeDims& d, int B, int np, int ir = 0) {
   const size_t nn = (size_t)d.n * d.n;
   const int ne = np > 0 ? np : 1;
   size_t b = (size_t)B * kBlocksPerSource * nn * sizeof(double2);
@@ -342,12 +362,14 @@ size_t plan_bytes(const ModeDims& d, int B, int np) {
   b += (size_t)B * (4 * d.N + 4 * d.N + 4) * sizeof(double2); // Kx Ky Kzr Kzt, V0, kinc
   b += (size_t)B * sizeof(SourceDev) + (size_t)3 * B * sizeof(uint32_t);
   b += (size_t)2 * B * d.n * sizeof(int);
+  if (ir > 0) b += zgesv_ir_ws_bytes(d.n, 2 * d.n, 2 * B, ir);
   b += 64 * 256;  // alignment slack
   return (b + 255) & ~(size_t)255;  // callers place further buffers right after the plan
 }
 
 int plan_take(rcwa_context* ctx, const ModeDims& d, int B, int np, Plan& pl) {
-  int rc = ctx_reserve(ctx, plan_bytes(d, B, np));
+  const int ir = active_ir_sweeps(ctx);
+  int rc = ctx_reserve(ctx, plan_bytes(d, B, np, ir));
   if (rc) return rc;
   char* w = (char*)ctx->ws;
   auto take = [&](size_t bytes) {
@@ -392,6 +414,12 @@ int plan_take(rcwa_context* ctx, const ModeDims& d, int B, int np, Plan& pl) {
   pl.src = (SourceDev*)take((size_t)B * sizeof(SourceDev));
   pl.st = (uint32_t*)take((size_t)3 * B * sizeof(uint32_t));
   pl.piv = (int*)take((size_t)2 * B * d.n * sizeof(int));
+  ctx->irws = nullptr;
+  ctx->irws_bytes = 0;
+  if (ir > 0) {
+    ctx->irws_bytes = zgesv_ir_ws_bytes(d.n, 2 * d.n, 2 * B, ir);
+    ctx->irws = take(ctx->irws_bytes);
+  }
   return RCWA_OK;
 }
 
@@ -490,6 +518,7 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   const long long nn = (long long)n * n;
   const long long s2 = 2 * nn, s3 = 3 * nn;
   const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
+  const int ltc = (ctx->tc & RCWA_MIXED_LAYER_GEMM) ? 1 : 0;
   int rc;
   // Q_i (:280-286) again (P is not needed past Omega^2)
   if ((rc = layer_pq(s, g, l, B, pl))) return rc;
@@ -508,12 +537,12 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   gm.B = pl.augWV; gm.ldb = n; gm.sB = s2;
   gm.C = augV; gm.ldc = n; gm.sC = s2;
   gm.dr = pl.ilam; gm.sdr = n;
-  gm.tc = ctx->tc;
+  gm.tc = ltc;
   if ((rc = zgemm(s, gm))) return rc;
   // W^-1, V^-1 (:335-336), one batched solve for both
   if ((rc = set_identity(s, pl.augWV, n, n, s2, 2 * n, n, 2 * B, one))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, n, pl.augWV, n, s2, 2 * B, pl.piv, pl.st, ctx->tc))) return rc;
+  if ((rc = lu_stage(ctx, RCWA_MIXED_LAYER_LU, n, n, pl.augWV, n, s2, 2 * B, pl.piv, pl.st))) return rc;
   if ((rc = fold_status(s, status, pl.st, B, 2))) return rc;
   // A = W^-1 W0 + V^-1 V0 -> s1, B -> s0 (:337-338)
   if ((rc = assemble_ab(s, B, d, pl.augWV + nn, s2, augV + nn, s2, pl.wv.V0, pl.s1, pl.s0))) return rc;
@@ -521,7 +550,7 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   if ((rc = copy_blocks(s, pl.augA, s2, pl.s1, nn, nn, B))) return rc;
   if ((rc = set_identity(s, pl.augA, n, n, s2, 2 * n, n, B, one))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, n, pl.augA, n, s2, B, pl.piv, pl.st, ctx->tc))) return rc;
+  if ((rc = lu_stage(ctx, RCWA_MIXED_LAYER_LU, n, n, pl.augA, n, s2, B, pl.piv, pl.st))) return rc;
   if ((rc = fold_status(s, status, pl.st, B, 1))) return rc;
   const double2* Ai = pl.augA + nn;
   // T1 = B A^-1 X -> s2   (X diag: column scaling)
@@ -531,7 +560,7 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   gm.B = Ai; gm.ldb = n; gm.sB = s2;
   gm.C = pl.s2; gm.ldc = n; gm.sC = nn;
   gm.dr = pl.X; gm.sdr = n;
-  gm.tc = ctx->tc;
+  gm.tc = ltc;
   if ((rc = zgemm(s, gm))) return rc;
   // D = A - X T1 B -> augD[0] (:346)
   if ((rc = copy_blocks(s, pl.augD, s3, pl.s1, nn, nn, B))) return rc;
@@ -542,14 +571,14 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   gm.B = pl.s0; gm.ldb = n; gm.sB = nn;
   gm.C = pl.augD; gm.ldc = n; gm.sC = s3;
   gm.dl = pl.X; gm.sdl = n;
-  gm.tc = ctx->tc;
+  gm.tc = ltc;
   if ((rc = zgemm(s, gm))) return rc;
   // R1 = X T1 A - B -> augD[1] (:347)
   if ((rc = copy_blocks(s, pl.augD + nn, s3, pl.s0, nn, nn, B))) return rc;
   gm.alpha = one; gm.beta = mone;
   gm.B = pl.s1;
   gm.C = pl.augD + nn;
-  gm.tc = ctx->tc;
+  gm.tc = ltc;
   if ((rc = zgemm(s, gm))) return rc;
   // T3 = A^-1 B -> s3 ; R2 = A - B T3 -> s1 (in place) (:348)
   gm = ZGemm();
@@ -557,19 +586,19 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   gm.A = Ai; gm.lda = n; gm.sA = s2;
   gm.B = pl.s0; gm.ldb = n; gm.sB = nn;
   gm.C = pl.s3; gm.ldc = n; gm.sC = nn;
-  gm.tc = ctx->tc;
+  gm.tc = ltc;
   if ((rc = zgemm(s, gm))) return rc;
   gm.alpha = mone; gm.beta = one;
   gm.A = pl.s0; gm.sA = nn;
   gm.B = pl.s3; gm.sB = nn;
   gm.C = pl.s1;
-  gm.tc = ctx->tc;
+  gm.tc = ltc;
   if ((rc = zgemm(s, gm))) return rc;
   // X R2 -> augD[2]; then [D | R1 | X R2] -> S11 = D^-1 R1 (:347), S12 = D^-1 X R2 (:348)
   if ((rc = scale_rows(s, pl.s1, n, n, n, nn, pl.X, n, B))) return rc;
   if ((rc = copy_blocks(s, pl.augD + 2 * nn, s3, pl.s1, nn, nn, B))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(pl.st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, 2 * n, pl.augD, n, s3, B, pl.piv, pl.st, ctx->tc))) return rc;
+  if ((rc = lu_stage(ctx, RCWA_MIXED_LAYER_LU, n, 2 * n, pl.augD, n, s3, B, pl.piv, pl.st))) return rc;
   (void)zero;
   return fold_status(s, status, pl.st, B, 1);
 }
@@ -597,10 +626,10 @@ int star_product_bd(rcwa_context* ctx, int B, const ModeDims& d, SMat& A, const 
   if ((rc = bd_apply(s, 1, N, n, n, L11, sL, A.p[3], n, A.s[3], augG, n, s3, mone, zero, 1, B))) return rc;
   if ((rc = copy_blocks(s, augG + nn, s3, A.p[2], A.s[2], nn, B))) return rc;
   if ((rc = copy_blocks(s, augG + 2 * nn, s3, A.p[3], A.s[3], nn, B))) return rc;
-  if ((rc = zgesv(s, n, 2 * n, augFG, n, s3, 2 * B, piv, st, ctx->tc))) return rc;
+  if ((rc = lu_stage(ctx, RCWA_MIXED_STAR_LU, n, 2 * n, augFG, n, s3, 2 * B, piv, st))) return rc;
   ZGemm g;
   g.m = n; g.n = n; g.k = n; g.batch = B;
-  g.tc = ctx->tc;
+  g.tc = (ctx->tc & RCWA_MIXED_STAR_GEMM) ? 1 : 0;
   // S11 = A11 + A12 X1
   g.alpha = one; g.beta = one;
   g.A = A.p[1]; g.lda = n; g.sA = A.s[1];
@@ -651,7 +680,7 @@ int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, c
     g.A = X; g.lda = n; g.sA = sX;
     g.B = Y; g.ldb = n; g.sB = sY;
     g.C = C; g.ldc = n; g.sC = sC;
-    g.tc = ctx->tc;
+    g.tc = (ctx->tc & RCWA_MIXED_STAR_GEMM) ? 1 : 0;
     return zgemm(s, g);
   };
   // [G1 | R22 D12 | R21 E] in augFG (stride 6n^2)
@@ -663,7 +692,7 @@ int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, c
   if ((rc = bd_apply(s, 1, N, n, n, R22, sP, D.p[0], n, D.s[0], augA, n, s2, mone, zero, 1, B))) return rc;
   if ((rc = gemm(n, 2, augA + nn, s2, D.p[0], D.s[0], u, s6, zero))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, n + 2, augFG, n, s6, B, piv, st, ctx->tc))) return rc;
+  if ((rc = lu_stage(ctx, RCWA_MIXED_STAR_LU, n, n + 2, augFG, n, s6, B, piv, st))) return rc;
   if ((rc = fold_status(s, status, st, B, 1))) return rc;
   // S'22 -> s0, S'21 E -> s1
   if ((rc = copy_blocks(s, s0, nn, D.p[3], D.s[3], nn, B))) return rc;
@@ -676,14 +705,14 @@ int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, c
   if ((rc = bd_apply(s, 1, N, n, n, T11, sP, s0, n, nn, augG2, n, s2, mone, zero, 1, B))) return rc;
   if ((rc = copy_blocks(s, augG2 + nn, s2, s1, nn, c2, B))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, 2, augWV, n, s2, 2 * B, piv, st, ctx->tc))) return rc;
+  if ((rc = lu_stage(ctx, RCWA_MIXED_STAR_LU, n, 2, augWV, n, s2, 2 * B, piv, st))) return rc;
   if ((rc = fold_status(s, status, st, B, 2))) return rc;
   // S''21 E = T21 z
   if ((rc = bd_apply(s, 0, N, n, 2, T21, sP, augG2 + nn, n, s2, S21E, n, c2, one, zero, 0, B))) return rc;
   // v = D11 R21 E + D12 x, then q = F1^-1 v
   if ((rc = gemm(n, 2, augA + nn, s2, D.p[1], D.s[1], augWV + nn, s2, one))) return rc;
   RCWA_CUDA_TRY(cudaMemsetAsync(st, 0, 3 * B * sizeof(uint32_t), s));
-  if ((rc = zgesv(s, n, 2, augA, n, s2, B, piv, st, ctx->tc))) return rc;
+  if ((rc = lu_stage(ctx, RCWA_MIXED_STAR_LU, n, 2, augA, n, s2, B, piv, st))) return rc;
   if ((rc = fold_status(s, status, st, B, 1))) return rc;
   // S''11 E = R11 E + R12 q
   if ((rc = bd_cols(s, N, a, R11, sP, S11E, n, c2, one, zero, B))) return rc;
@@ -692,7 +721,9 @@ int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, c
 
 }  // namespace
 
-size_t sweep_bytes_per_source(const ModeDims& d, int np) { return plan_bytes(d, 1, np); }
+size_t sweep_bytes_per_source(const ModeDims& d, int np, int ir_sweeps) {
+  return plan_bytes(d, 1, np, ir_sweeps);
+}
 
 // The layer set of one geometry, shared by every solve of a sweep.
 Layers layers_of(const rcwa_geometry* g) {
@@ -871,7 +902,7 @@ int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* s
     rcwa_context* c;
     ~TcScope() { c->tc = 0; }
   } tc_scope{ctx};
-  ctx->tc = precision == RCWA_PREC_MIXED ? 1 : 0;
+  ctx->tc = precision == RCWA_PREC_MIXED ? ctx->mixed_stages : 0u;
   const ModeDims& d = g->d;
   // chunk size from the memory budget
   size_t budget = ctx->mem_budget;
@@ -882,7 +913,7 @@ int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* s
   }
   int np = 0;
   for (int l = 0; l < g->nl; ++l) np += g->uniform[l] ? 0 : 1;
-  const size_t per = plan_bytes(d, 1, np);
+  const size_t per = plan_bytes(d, 1, np, active_ir_sweeps(ctx));
   int chunk = (int)std::max<size_t>(1, budget / per);
   chunk = std::min(chunk, B);
   const Layers G = layers_of(g);

@@ -20,10 +20,16 @@ struct rcwa_context {
   size_t pinned_bytes = 0;
   uint64_t launches_at_create = 0;
   size_t mem_budget = 0;  // bytes usable for one sweep chunk (0 = auto)
-  // 1 while a mixed-precision sweep runs: the S-matrix algebra (layer
-  // assembly, star products, their LU solves) uses split-TF32 tensor-core
-  // GEMMs; Omega^2 and the eigensolver stay FP64
-  int tc = 0;
+  // RCWA_MIXED_* stages active in the running solve: mixed_stages while a
+  // mixed-precision sweep runs, 0 otherwise.  GEMM stages use split-TF32
+  // tensor-core GEMMs, LU stages an FP32 LU with ir_sweeps FP64 refinement
+  // sweeps; Omega^2 and the eigensolver stay FP64
+  unsigned tc = 0;
+  unsigned mixed_stages = RCWA_MIXED_ALL;
+  int ir_sweeps = 1;
+  // refinement workspace of the current sweep chunk (inside ws), see zgesv_ir
+  void* irws = nullptr;
+  size_t irws_bytes = 0;
   // worker contexts (own stream + workspace) that run independent group
   // chunks of rcwa_solve_batch concurrently; owned by this context
   std::vector<rcwa_context*> workers;
@@ -115,8 +121,12 @@ int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* s
                  int precision, double* R, double* T, double* tot, uint32_t* status);
 
 // Bytes of device workspace per source for a sweep at this size with np
-// patterned layers.
-size_t sweep_bytes_per_source(const ModeDims& d, int np);
+// patterned layers; ir_sweeps > 0 adds the refinement workspace of the
+// mixed-precision LU stages.
+size_t sweep_bytes_per_source(const ModeDims& d, int np, int ir_sweeps = 0);
+// ir_sweeps of a context's running solve: its refinement sweeps when an LU
+// stage runs mixed, else 0.
+int active_ir_sweeps(const rcwa_context* ctx);
 
 // Dense building blocks on device pointers (used by the step-level ABI).
 struct SMat {

@@ -1,11 +1,12 @@
-// Batched complex128 linear solve X = A^-1 B by LU with partial pivoting.
+// Batched complex linear solve X = A^-1 B by LU with partial pivoting.
 //
 // This replaces every Eigen ``.lu().solve(...)`` (PartialPivLU) of the
 // reference (rcwa.cpp:267, 270, 280, 281, 335, 336, 345-348, 392-408,
 // 453-462, 520, 605-611).  The system is stored as one augmented column-major
-// block M = [A | B] (n rows, n + nrhs columns); on return the A part holds U
-// (and the L multipliers) and the B part holds the solution.
+// block M = [A | B] (n rows, n + nrhs columns); on return the B part holds
+// the solution.
 //
+// FP64 form (zgesv):
 // 1. P A = L U by blocked right-looking elimination over the A columns, with
 //    panel width NB:
 //      panel  : one CTA per matrix factors the n-j x NB panel (pivot search,
@@ -23,6 +24,17 @@
 //    column kernels.  With many right-hand sides (the [A | I] and [D | R | R']
 //    systems of the S-matrix algebra) this moves most of the flops from
 //    rank-NB updates onto large-k GEMMs.
+// On return the A part holds U and the L multipliers.
+//
+// Mixed-precision form (zgesv_ir): the same factorisation and solves run on
+// a complex64 copy of [A | B] (the kernels below are templates over the
+// element type; the FP32 GEMM updates run on CUDA cores), giving X0.  Then
+// each refinement sweep computes the residual R = B - A X in FP64 on the
+// FP64 tensor cores (the DMMA GEMM, A read from the untouched FP64 A part),
+// solves L U dX = P R with the FP32 factors and adds dX to X in FP64.  A
+// solve whose last correction stays above 1e-4 of |X| is flagged
+// RCWA_STATUS_REFINE_SLOW (the FP32 factors were too inaccurate for the
+// sweeps run).  The A part is left unchanged.
 #include <algorithm>
 #include <functional>
 
@@ -37,11 +49,25 @@ constexpr int NB = 32;
 constexpr int PANEL_NT = 256;
 constexpr int COL_NT = 64;
 
-__device__ __forceinline__ void argmax_reduce(double& v, int& idx) {
+template <class T>
+struct Cx;
+template <>
+struct Cx<double2> {
+  using R = double;
+  __host__ __device__ static double2 mk(double r, double i) { return make_double2(r, i); }
+};
+template <>
+struct Cx<float2> {
+  using R = float;
+  __host__ __device__ static float2 mk(float r, float i) { return make_float2(r, i); }
+};
+
+template <class R>
+__device__ __forceinline__ void argmax_reduce(R& v, int& idx) {
   // warp-level: keep the larger value, ties -> smaller index
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
-    double ov = __shfl_down_sync(0xffffffffu, v, off);
+    R ov = __shfl_down_sync(0xffffffffu, v, off);
     int oi = __shfl_down_sync(0xffffffffu, idx, off);
     if (ov > v || (ov == v && oi < idx)) {
       v = ov;
@@ -50,33 +76,35 @@ __device__ __forceinline__ void argmax_reduce(double& v, int& idx) {
   }
 }
 
+template <class T>
 __global__ void __launch_bounds__(PANEL_NT)
-lu_panel_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int j, int jb,
+lu_panel_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int j, int jb,
                 int* __restrict__ pivg, uint32_t* __restrict__ status) {
+  using R = typename Cx<T>::R;
   const int b = blockIdx.x;
-  double2* M = Mg + (long long)b * stride;
+  T* M = Mg + (long long)b * stride;
   int* piv = pivg + (long long)b * n;
-  __shared__ double s_val[PANEL_NT / 32];
+  __shared__ R s_val[PANEL_NT / 32];
   __shared__ int s_idx[PANEL_NT / 32];
-  __shared__ double2 s_urow[NB];
+  __shared__ T s_urow[NB];
   __shared__ int s_p;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
   for (int c = 0; c < jb; ++c) {
     const int col = j + c;
-    double2* Mc = M + (long long)col * ld;
+    T* Mc = M + (long long)col * ld;
     // 1. pivot search over rows col..n-1 (|re|+|im|, first maximum wins)
-    double best = -1.0;
+    R best = -1;
     int bi = n;
     for (int r = col + tid; r < n; r += PANEL_NT) {
-      double v = cabs1(Mc[r]);
+      R v = cabs1(Mc[r]);
       if (v > best) { best = v; bi = r; }
     }
     argmax_reduce(best, bi);
     if (lane == 0) { s_val[wid] = best; s_idx[wid] = bi; }
     __syncthreads();
     if (wid == 0) {
-      best = lane < PANEL_NT / 32 ? s_val[lane] : -1.0;
+      best = lane < PANEL_NT / 32 ? s_val[lane] : R(-1);
       bi = lane < PANEL_NT / 32 ? s_idx[lane] : n;
       argmax_reduce(best, bi);
       if (lane == 0) {
@@ -90,8 +118,8 @@ lu_panel_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int j
     // 2. swap rows col <-> p inside the panel
     if (p != col) {
       for (int cc = tid; cc < jb; cc += PANEL_NT) {
-        double2* q = M + (long long)(j + cc) * ld;
-        double2 t = q[col];
+        T* q = M + (long long)(j + cc) * ld;
+        T t = q[col];
         q[col] = q[p];
         q[p] = t;
       }
@@ -99,18 +127,18 @@ lu_panel_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int j
     __syncthreads();
     // 3. pivot row of the remaining panel columns -> smem
     for (int cc = c + 1 + tid; cc < jb; cc += PANEL_NT) s_urow[cc] = M[(long long)(j + cc) * ld + col];
-    const double2 pv = Mc[col];
-    if (tid == 0 && pv.x == 0.0 && pv.y == 0.0) atomicOr(status + b, (unsigned)ST_SINGULAR);
+    const T pv = Mc[col];
+    if (tid == 0 && pv.x == R(0) && pv.y == R(0)) atomicOr(status + b, (unsigned)ST_SINGULAR);
     __syncthreads();
-    const double2 inv = crcp(pv);
+    const T inv = crcp(pv);
     // 4. scale the column below the pivot and rank-1 update the panel
     for (int r = col + 1 + tid; r < n; r += PANEL_NT) {
-      double2 l = cmul(Mc[r], inv);
+      T l = cmul(Mc[r], inv);
       Mc[r] = l;
       for (int cc = c + 1; cc < jb; ++cc) {
-        double2* q = M + (long long)(j + cc) * ld + r;
-        double2 u = s_urow[cc];
-        double2 v = *q;
+        T* q = M + (long long)(j + cc) * ld + r;
+        T u = s_urow[cc];
+        T v = *q;
         v.x -= l.x * u.x - l.y * u.y;
         v.y -= l.x * u.y + l.y * u.x;
         *q = v;
@@ -122,13 +150,14 @@ lu_panel_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int j
 
 // Row swaps of panel j plus forward substitution with the unit-lower L11 for
 // columns [c_begin, c_end) of the augmented matrix.
+template <class T>
 __global__ void __launch_bounds__(COL_NT)
-lu_swap_lsolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int j, int jb,
-                      int c_begin, int c_end, const int* __restrict__ pivg, int swap) {
+lu_swap_lsolve_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int j, int jb, int c_begin,
+                      int c_end, const int* __restrict__ pivg, int swap) {
   const int b = blockIdx.y;
-  double2* M = Mg + (long long)b * stride;
+  T* M = Mg + (long long)b * stride;
   const int* piv = pivg + (long long)b * n;
-  __shared__ double2 L[NB][NB + 1];  // L[r][c]
+  __shared__ T L[NB][NB + 1];  // L[r][c]
   __shared__ int sp[NB];
   const int tid = threadIdx.x;
   for (int e = tid; e < jb * jb; e += COL_NT) {
@@ -140,25 +169,25 @@ lu_swap_lsolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int n,
   __syncthreads();
   const int col = c_begin + blockIdx.x * COL_NT + tid;
   if (col >= c_end) return;
-  double2* q = M + (long long)col * ld;
+  T* q = M + (long long)col * ld;
   if (swap)
     for (int c = 0; c < jb; ++c) {
       int p = sp[c];
       if (p != j + c) {
-        double2 t = q[j + c];
+        T t = q[j + c];
         q[j + c] = q[p];
         q[p] = t;
       }
     }
-  double2 x[NB];
+  T x[NB];
 #pragma unroll
-  for (int c = 0; c < NB; ++c) x[c] = (c < jb) ? q[j + c] : cmk(0.0, 0.0);
+  for (int c = 0; c < NB; ++c) x[c] = (c < jb) ? q[j + c] : Cx<T>::mk(0, 0);
 #pragma unroll
   for (int c = 0; c < NB; ++c) {
 #pragma unroll
     for (int r = c + 1; r < NB; ++r) {
       if (r < jb) {
-        double2 l = L[r][c];
+        T l = L[r][c];
         x[r].x -= l.x * x[c].x - l.y * x[c].y;
         x[r].y -= l.x * x[c].y + l.y * x[c].x;
       }
@@ -170,21 +199,21 @@ lu_swap_lsolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int n,
 }
 
 // Row interchanges piv[r_begin..r_end) (in order) applied to columns
-// [c_begin, c_end): the multipliers left of a panel, and the right-hand sides
-// (B <- P B).
+// [c_begin, c_end): the multipliers left of a panel.
+template <class T>
 __global__ void __launch_bounds__(COL_NT)
-lu_rowswap_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int r_begin, int r_end,
+lu_rowswap_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int r_begin, int r_end,
                   int c_begin, int c_end, const int* __restrict__ pivg) {
   const int b = blockIdx.y;
-  double2* M = Mg + (long long)b * stride;
+  T* M = Mg + (long long)b * stride;
   const int* piv = pivg + (long long)b * n;
   const int col = c_begin + blockIdx.x * COL_NT + threadIdx.x;
   if (col >= c_end) return;
-  double2* q = M + (long long)col * ld;
+  T* q = M + (long long)col * ld;
   for (int r = r_begin; r < r_end; ++r) {
     const int p = piv[r];
     if (p != r) {
-      const double2 t = q[r];
+      const T t = q[r];
       q[r] = q[p];
       q[p] = t;
     }
@@ -216,19 +245,22 @@ __global__ void lu_perm_kernel(int* __restrict__ pivg, int n) {
 // column in shared memory (coalesced read) and writes it back permuted
 // (coalesced write); PERM_CPW columns per warp.
 constexpr int PERM_WARPS = 8, PERM_CPW = 4;
+constexpr int GATHER_SMEM = 200 * 1024;
+template <class T>
 __global__ void __launch_bounds__(PERM_WARPS * 32)
-lu_gather_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int c_begin, int c_end,
+lu_gather_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int c_begin, int c_end,
                  const int* __restrict__ idxg) {
-  extern __shared__ double2 col_sh[];
-  const int nw = blockDim.x >> 5;   // warps (fewer for large n: n doubles2 of shared memory each)
+  extern __shared__ __align__(16) unsigned char gather_raw[];
+  T* col_sh = reinterpret_cast<T*>(gather_raw);
+  const int nw = blockDim.x >> 5;   // warps (fewer for large n: n elements of shared memory each)
   const int b = blockIdx.y, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double2* M = Mg + (long long)b * stride;
+  T* M = Mg + (long long)b * stride;
   const int* idx = idxg + (long long)b * n;
-  double2* sh = col_sh + (size_t)w * n;
+  T* sh = col_sh + (size_t)w * n;
   for (int t = 0; t < PERM_CPW; ++t) {
     const int col = c_begin + (blockIdx.x * nw + w) * PERM_CPW + t;
     if (col >= c_end) break;   // warp-uniform
-    double2* q = M + (long long)col * ld;
+    T* q = M + (long long)col * ld;
     for (int r = lane; r < n; r += 32) sh[r] = q[r];
     __syncwarp();
     for (int r = lane; r < n; r += 32) q[r] = sh[idx[r]];
@@ -238,13 +270,13 @@ lu_gather_kernel(double2* __restrict__ Mg, int ld, long long stride, int n, int 
 
 // Upper-triangular solve X = U11^-1 X for rows j..j+jb-1 of the right-hand
 // side columns [c_begin, c_end).
+template <class T>
 __global__ void __launch_bounds__(COL_NT)
-lu_usolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int j, int jb, int c_begin,
-                 int c_end) {
+lu_usolve_kernel(T* __restrict__ Mg, int ld, long long stride, int j, int jb, int c_begin, int c_end) {
   const int b = blockIdx.y;
-  double2* M = Mg + (long long)b * stride;
-  __shared__ double2 U[NB][NB + 1];
-  __shared__ double2 dinv[NB];
+  T* M = Mg + (long long)b * stride;
+  __shared__ T U[NB][NB + 1];
+  __shared__ T dinv[NB];
   const int tid = threadIdx.x;
   for (int e = tid; e < jb * jb; e += COL_NT) {
     int r = e % jb, c = e / jb;
@@ -255,17 +287,17 @@ lu_usolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int j, int 
   __syncthreads();
   const int col = c_begin + blockIdx.x * COL_NT + tid;
   if (col >= c_end) return;
-  double2* q = M + (long long)col * ld;
-  double2 x[NB];
+  T* q = M + (long long)col * ld;
+  T x[NB];
 #pragma unroll
-  for (int c = 0; c < NB; ++c) x[c] = (c < jb) ? q[j + c] : cmk(0.0, 0.0);
+  for (int c = 0; c < NB; ++c) x[c] = (c < jb) ? q[j + c] : Cx<T>::mk(0, 0);
 #pragma unroll
   for (int c = NB - 1; c >= 0; --c) {
     if (c < jb) {
       x[c] = cmul(x[c], dinv[c]);
 #pragma unroll
       for (int r = 0; r < c; ++r) {
-        double2 u = U[r][c];
+        T u = U[r][c];
         x[r].x -= u.x * x[c].x - u.y * x[c].y;
         x[r].y -= u.x * x[c].y + u.y * x[c].x;
       }
@@ -276,93 +308,221 @@ lu_usolve_kernel(double2* __restrict__ Mg, int ld, long long stride, int j, int 
     if (c < jb) q[j + c] = x[c];
 }
 
-}  // namespace
+// ---------------------------------------------------------------------------
+// complex64 update C -= A B on CUDA cores (the FP32 factorisation's trailing
+// updates and triangular-solve blocks).  64 x 64 C tile, K step 16, 256
+// threads as 16 x 16, each a 4 x 4 complex micro-tile; the next K tile is
+// fetched into registers while the current one is consumed from shared
+// memory.
+// ---------------------------------------------------------------------------
+constexpr int CT = 64, CK = 16, CNT = 256;
 
-int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch,
-          int* piv, uint32_t* status, int tc) {
-  if (n <= 0 || batch <= 0) return RCWA_OK;
-  const int ncols = n + nrhs;
-  auto gemm = [&](int m, int nc, int k, const double2* A, const double2* Bm, double2* C) {
-    ZGemm gm;
-    gm.m = m;
-    gm.n = nc;
-    gm.k = k;
-    gm.alpha = cmk(-1.0, 0.0);
-    gm.beta = cmk(1.0, 0.0);
-    gm.A = A;
-    gm.lda = ld;
-    gm.sA = stride;
-    gm.B = Bm;
-    gm.ldb = ld;
-    gm.sB = stride;
-    gm.C = C;
-    gm.ldc = ld;
-    gm.sC = stride;
-    gm.batch = batch;
-    gm.tc = tc;
-    return zgemm(s, gm);
+__global__ void __launch_bounds__(CNT)
+cgemm_sub_kernel(int m, int n, int k, const float2* __restrict__ A, int lda, long long sA,
+                 const float2* __restrict__ B, int ldb, long long sB, float2* __restrict__ C, int ldc,
+                 long long sC) {
+  __shared__ float2 As[2][CK][CT];
+  __shared__ float2 Bs[2][CK][CT + 1];
+  const int bz = blockIdx.z;
+  A += (long long)bz * sA;
+  B += (long long)bz * sB;
+  C += (long long)bz * sC;
+  const int m0 = blockIdx.y * CT, n0 = blockIdx.x * CT;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  float2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = make_float2(0.f, 0.f);
+  float2 ra[4], rb[4];
+  auto gload = [&](int k0) {
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const int e = tid + h * CNT, r = e & (CT - 1), kk = e >> 6;
+      const int gr = m0 + r, gk = k0 + kk;
+      ra[h] = (gr < m && gk < k) ? A[(long long)gk * lda + gr] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const int e = tid + h * CNT, kk = e & (CK - 1), c = e >> 4;
+      const int gk = k0 + kk, gc = n0 + c;
+      rb[h] = (gk < k && gc < n) ? B[(long long)gc * ldb + gk] : make_float2(0.f, 0.f);
+    }
   };
-  // 1. P A = L U, right-looking over the A columns only
+  auto sstore = [&](int buf) {
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const int e = tid + h * CNT;
+      As[buf][e >> 6][e & (CT - 1)] = ra[h];
+      Bs[buf][e & (CK - 1)][e >> 4] = rb[h];
+    }
+  };
+  const int kt = (k + CK - 1) / CK;
+  if (kt > 0) {
+    gload(0);
+    sstore(0);
+  }
+  __syncthreads();
+  for (int t = 0; t < kt; ++t) {
+    const int buf = t & 1;
+    if (t + 1 < kt) gload((t + 1) * CK);
+#pragma unroll
+    for (int kk = 0; kk < CK; ++kk) {
+      float2 a[4], bb[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bb[j] = Bs[buf][kk][ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[i][j].x = fmaf(a[i].x, bb[j].x, fmaf(-a[i].y, bb[j].y, acc[i][j].x));
+          acc[i][j].y = fmaf(a[i].x, bb[j].y, fmaf(a[i].y, bb[j].x, acc[i][j].y));
+        }
+    }
+    if (t + 1 < kt) sstore(buf ^ 1);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int col = n0 + ty + 16 * j;
+    if (col >= n) continue;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int row = m0 + tx + 16 * i;
+      if (row >= m) continue;
+      float2* cp = C + (long long)col * ldc + row;
+      float2 v = *cp;
+      v.x -= acc[i][j].x;
+      v.y -= acc[i][j].y;
+      *cp = v;
+    }
+  }
+}
+
+// C -= A B, batched (FP64: the DMMA / CUDA-core ZGEMM; FP32: cgemm_sub_kernel)
+int gemm_sub(cudaStream_t s, int m, int nc, int k, const double2* A, int ld, long long stride,
+             const double2* Bm, double2* C, int batch) {
+  ZGemm gm;
+  gm.m = m;
+  gm.n = nc;
+  gm.k = k;
+  gm.alpha = cmk(-1.0, 0.0);
+  gm.beta = cmk(1.0, 0.0);
+  gm.A = A;
+  gm.lda = ld;
+  gm.sA = stride;
+  gm.B = Bm;
+  gm.ldb = ld;
+  gm.sB = stride;
+  gm.C = C;
+  gm.ldc = ld;
+  gm.sC = stride;
+  gm.batch = batch;
+  return zgemm(s, gm);
+}
+int gemm_sub(cudaStream_t s, int m, int nc, int k, const float2* A, int ld, long long stride,
+             const float2* Bm, float2* C, int batch) {
+  if (m <= 0 || nc <= 0 || batch <= 0) return RCWA_OK;
+  dim3 g(cdiv_up(nc, CT), cdiv_up(m, CT), batch);
+  void* tok = prof_begin(s);
+  cgemm_sub_kernel<<<g, CNT, 0, s>>>(m, nc, k, A, ld, stride, Bm, ld, stride, C, ld, stride);
+  prof_end(s, tok, "cgemm_f32");
+  if (tok) prof_add_flops("cgemm_f32", 8.0 * m * (double)nc * (double)k * batch);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  return RCWA_OK;
+}
+
+// Dynamic shared-memory limits of the permutation kernels, set once per
+// device to their bound (concurrent callers with different n never lower it).
+int perm_attrs() {
+  static bool set[64] = {};
+  int dev = 0;
+  RCWA_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 64 || !set[dev]) {
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(lu_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(lu_gather_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       GATHER_SMEM));
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(lu_gather_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       GATHER_SMEM));
+    if (dev < 64) set[dev] = true;
+  }
+  return RCWA_OK;
+}
+
+// 1. P A = L U on the A part of the augmented M, right-looking over the A
+// columns only (piv receives the interchanges).
+template <class T>
+int lu_factor(cudaStream_t s, int n, T* M, int ld, long long stride, int batch, int* piv,
+              uint32_t* status) {
   for (int j = 0; j < n; j += NB) {
     const int jb = (n - j < NB) ? (n - j) : NB;
     void* tok = prof_begin(s);
-    lu_panel_kernel<<<batch, PANEL_NT, 0, s>>>(M, ld, stride, n, j, jb, piv, status);
+    lu_panel_kernel<T><<<batch, PANEL_NT, 0, s>>>(M, ld, stride, n, j, jb, piv, status);
     prof_end(s, tok, "lu_panel");
     count_launch();
     RCWA_LAUNCH_CHECK();
     if (j > 0) {   // the earlier multipliers follow this panel's interchanges (P A = L U)
       dim3 g(cdiv_up(j, COL_NT), batch);
-      lu_rowswap_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, j + jb, 0, j, piv);
+      lu_rowswap_kernel<T><<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, j + jb, 0, j, piv);
       count_launch();
       RCWA_LAUNCH_CHECK();
     }
     const int cb = j + jb;
     if (cb < n) {
       dim3 g(cdiv_up(n - cb, COL_NT), batch);
-      lu_swap_lsolve_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, jb, cb, n, piv, 1);
+      lu_swap_lsolve_kernel<T><<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, jb, cb, n, piv, 1);
       count_launch();
       RCWA_LAUNCH_CHECK();
-      int rc = gemm(n - cb, n - cb, jb, M + (long long)j * ld + cb, M + (long long)cb * ld + j,
-                    M + (long long)cb * ld + cb);
+      int rc = gemm_sub(s, n - cb, n - cb, jb, M + (long long)j * ld + cb, ld, stride,
+                        M + (long long)cb * ld + j, M + (long long)cb * ld + cb, batch);
       if (rc) return rc;
     }
   }
+  return RCWA_OK;
+}
+
+// The interchanges in piv composed into gather indices (overwrites piv).
+int lu_compose(cudaStream_t s, int n, int* piv, int batch) {
+  int rc = perm_attrs();
+  if (rc) return rc;
+  lu_perm_kernel<<<batch, 128, (size_t)n * sizeof(int), s>>>(piv, n);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  return RCWA_OK;
+}
+
+// 2.-4. X = U^-1 L^-1 P B for the nrhs columns that follow the A part of M,
+// with the gather indices of lu_compose.
+template <class T>
+int lu_solve(cudaStream_t s, int n, int nrhs, T* M, int ld, long long stride, int batch, const int* idx) {
   if (nrhs <= 0) return RCWA_OK;
-  // 2. B <- P B
-  double2* Bc = M + (long long)n * ld;   // right-hand sides, rows 0..n-1
+  const int ncols = n + nrhs;
+  T* Bc = M + (long long)n * ld;   // right-hand sides, rows 0..n-1
   {
-    const size_t pshm = (size_t)n * sizeof(int);
-    const int pw = (int)std::min<size_t>(PERM_WARPS, (200 * 1024) / ((size_t)n * sizeof(double2)));
+    const int pw = (int)std::min<size_t>(PERM_WARPS, GATHER_SMEM / ((size_t)n * sizeof(T)));
     if (pw < 1) {
       set_last_error("zgesv: n=%d too large", n);
       return RCWA_ERR_INVALID;
     }
-    const size_t gshm = (size_t)pw * n * sizeof(double2);
-    static bool set[64] = {};   // per device: allow the bound once
-    int dev = 0;
-    RCWA_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev >= 64 || !set[dev]) {
-      RCWA_CUDA_TRY(cudaFuncSetAttribute(lu_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-      RCWA_CUDA_TRY(cudaFuncSetAttribute(lu_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-      if (dev < 64) set[dev] = true;
-    }
-    lu_perm_kernel<<<batch, 128, pshm, s>>>(piv, n);   // piv now holds the gather indices
-    count_launch();
-    RCWA_LAUNCH_CHECK();
+    int rc = perm_attrs();
+    if (rc) return rc;
+    const size_t gshm = (size_t)pw * n * sizeof(T);
     dim3 g(cdiv_up(nrhs, pw * PERM_CPW), batch);
-    lu_gather_kernel<<<g, pw * 32, gshm, s>>>(M, ld, stride, n, n, ncols, piv);
+    lu_gather_kernel<T><<<g, pw * 32, gshm, s>>>(M, ld, stride, n, n, ncols, idx);
     count_launch();
     RCWA_LAUNCH_CHECK();
   }
-  // 3./4. L Y = P B, then U X = Y, by recursive halving: the off-diagonal
-  // blocks become GEMMs with k up to n/2 (tensor-core sized), only the
-  // diagonal NB x NB blocks are solved by the column kernels
+  // L Y = P B, then U X = Y, by recursive halving: the off-diagonal blocks
+  // become GEMMs with k up to n/2, only the diagonal NB x NB blocks are
+  // solved by the column kernels
   auto split = [](int r0, int r1) { return r0 + NB * (((r1 - r0 + NB - 1) / NB) / 2); };
-  int rc = RCWA_OK;
   std::function<int(int, int)> lower = [&](int r0, int r1) -> int {
     if (r1 - r0 <= NB) {
       dim3 g(cdiv_up(nrhs, COL_NT), batch);
-      lu_swap_lsolve_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, n, r0, r1 - r0, n, ncols, piv, 0);
+      lu_swap_lsolve_kernel<T><<<g, COL_NT, 0, s>>>(M, ld, stride, n, r0, r1 - r0, n, ncols, idx, 0);
       count_launch();
       RCWA_LAUNCH_CHECK();
       return RCWA_OK;
@@ -370,14 +530,15 @@ int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride,
     const int mid = split(r0, r1);
     int r = lower(r0, mid);
     if (r) return r;
-    r = gemm(r1 - mid, nrhs, mid - r0, M + (long long)r0 * ld + mid, Bc + r0, Bc + mid);
+    r = gemm_sub(s, r1 - mid, nrhs, mid - r0, M + (long long)r0 * ld + mid, ld, stride, Bc + r0, Bc + mid,
+                 batch);
     if (r) return r;
     return lower(mid, r1);
   };
   std::function<int(int, int)> upper = [&](int r0, int r1) -> int {
     if (r1 - r0 <= NB) {
       dim3 g(cdiv_up(nrhs, COL_NT), batch);
-      lu_usolve_kernel<<<g, COL_NT, 0, s>>>(M, ld, stride, r0, r1 - r0, n, ncols);
+      lu_usolve_kernel<T><<<g, COL_NT, 0, s>>>(M, ld, stride, r0, r1 - r0, n, ncols);
       count_launch();
       RCWA_LAUNCH_CHECK();
       return RCWA_OK;
@@ -385,12 +546,213 @@ int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride,
     const int mid = split(r0, r1);
     int r = upper(mid, r1);
     if (r) return r;
-    r = gemm(mid - r0, nrhs, r1 - mid, M + (long long)mid * ld + r0, Bc + mid, Bc + r0);
+    r = gemm_sub(s, mid - r0, nrhs, r1 - mid, M + (long long)mid * ld + r0, ld, stride, Bc + mid, Bc + r0,
+                 batch);
     if (r) return r;
     return upper(r0, mid);
   };
-  if ((rc = lower(0, n))) return rc;
+  int rc = lower(0, n);
+  if (rc) return rc;
   return upper(0, n);
+}
+
+// ---------------------------------------------------------------------------
+// refinement kernels (one grid row per system, grid-stride over its entries)
+// ---------------------------------------------------------------------------
+constexpr int IR_NT = 256;
+
+// Mf[:, 0:ncols] = (complex64) M[:, 0:ncols]  (Mf: ld n, stride sf)
+__global__ void ir_to_f32_kernel(const double2* __restrict__ Mg, int ld, long long stride,
+                                 float2* __restrict__ Mf, long long sf, int n, int ncols) {
+  const int b = blockIdx.y;
+  const double2* M = Mg + (long long)b * stride;
+  float2* F = Mf + (long long)b * sf;
+  const long long total = (long long)n * ncols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e / n), r = (int)(e - (long long)c * n);
+    const double2 v = M[(long long)c * ld + r];
+    F[e] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+// X0 from the FP32 solve: R = B (FP64 right-hand sides of M), B <- (FP64) Xf
+__global__ void ir_take_x0_kernel(double2* __restrict__ Mg, int ld, long long stride,
+                                  double2* __restrict__ Rg, const float2* __restrict__ Xf, long long sf,
+                                  int n, int nrhs) {
+  const int b = blockIdx.y;
+  double2* Bm = Mg + (long long)b * stride + (long long)n * ld;
+  double2* R = Rg + (long long)b * n * nrhs;
+  const float2* X = Xf + (long long)b * sf;
+  const long long total = (long long)n * nrhs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e / n), r = (int)(e - (long long)c * n);
+    double2* bp = Bm + (long long)c * ld + r;
+    R[e] = *bp;
+    const float2 x = X[e];
+    *bp = make_double2((double)x.x, (double)x.y);
+  }
+}
+
+// Xf = (complex64) R
+__global__ void ir_residual_f32_kernel(const double2* __restrict__ Rg, float2* __restrict__ Xf, long long sf,
+                                       int n, int nrhs) {
+  const int b = blockIdx.y;
+  const double2* R = Rg + (long long)b * n * nrhs;
+  float2* X = Xf + (long long)b * sf;
+  const long long total = (long long)n * nrhs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const double2 v = R[e];
+    X[e] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+// B <- B + (FP64) dXf; D (optional) <- (FP64) dXf; nrm[b] = (max |dX|, max |X|)
+// as order-preserving bits of non-negative floats
+__global__ void __launch_bounds__(IR_NT)
+ir_update_kernel(double2* __restrict__ Mg, int ld, long long stride, const float2* __restrict__ Xf,
+                 long long sf, double2* __restrict__ Dg, int n, int nrhs, unsigned* __restrict__ nrm) {
+  const int b = blockIdx.y;
+  double2* Bm = Mg + (long long)b * stride + (long long)n * ld;
+  const float2* X = Xf + (long long)b * sf;
+  double2* D = Dg ? Dg + (long long)b * n * nrhs : nullptr;
+  const long long total = (long long)n * nrhs;
+  float mdx = 0.f, mx = 0.f;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e / n), r = (int)(e - (long long)c * n);
+    const float2 d = X[e];
+    double2* bp = Bm + (long long)c * ld + r;
+    double2 v = *bp;
+    v.x += (double)d.x;
+    v.y += (double)d.y;
+    *bp = v;
+    if (D) D[e] = make_double2((double)d.x, (double)d.y);
+    mdx = fmaxf(mdx, fabsf(d.x) + fabsf(d.y));
+    mx = fmaxf(mx, (float)(fabs(v.x) + fabs(v.y)));
+  }
+  // NaN never wins fmaxf; a non-finite solve is caught by the efficiency checks
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    mdx = fmaxf(mdx, __shfl_down_sync(0xffffffffu, mdx, off));
+    mx = fmaxf(mx, __shfl_down_sync(0xffffffffu, mx, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(nrm + 2 * b, __float_as_uint(mdx));
+    atomicMax(nrm + 2 * b + 1, __float_as_uint(mx));
+  }
+}
+
+__global__ void ir_flag_kernel(const unsigned* __restrict__ nrm, uint32_t* __restrict__ status, int batch,
+                               float tol) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  const float dx = __uint_as_float(nrm[2 * b]), x = __uint_as_float(nrm[2 * b + 1]);
+  if (dx > tol * x) status[b] |= RCWA_STATUS_REFINE_SLOW;
+}
+
+size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+unsigned ir_grid_x(long long per_system) {
+  const long long g = (per_system + IR_NT - 1) / IR_NT;
+  return (unsigned)std::min<long long>(std::max<long long>(g, 1), 64);
+}
+
+}  // namespace
+
+int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch, int* piv,
+          uint32_t* status) {
+  if (n <= 0 || batch <= 0) return RCWA_OK;
+  int rc = lu_factor<double2>(s, n, M, ld, stride, batch, piv, status);
+  if (rc || nrhs <= 0) return rc;
+  if ((rc = lu_compose(s, n, piv, batch))) return rc;   // piv now holds the gather indices
+  return lu_solve<double2>(s, n, nrhs, M, ld, stride, batch, piv);
+}
+
+size_t zgesv_ir_ws_bytes(int n, int nrhs, int batch, int sweeps) {
+  if (n <= 0 || batch <= 0) return 0;
+  const size_t sys = (size_t)batch * n;
+  size_t b = al256(sys * (size_t)(n + nrhs) * sizeof(float2));    // complex64 [A | B]
+  b += al256(sys * (size_t)nrhs * sizeof(double2));                // FP64 residual
+  if (sweeps > 1) b += al256(sys * (size_t)nrhs * sizeof(double2));  // FP64 correction
+  b += al256((size_t)batch * 2 * sizeof(unsigned));
+  return b + 256;
+}
+
+int zgesv_ir(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch, int* piv,
+             uint32_t* status, void* ws, int sweeps) {
+  if (n <= 0 || batch <= 0) return RCWA_OK;
+  if (sweeps < 1) sweeps = 1;
+  const long long sf = (long long)n * (n + nrhs);
+  const long long sr = (long long)n * nrhs;
+  char* w = (char*)(((uintptr_t)ws + 255) & ~(uintptr_t)255);
+  float2* Mf = (float2*)w;
+  w += al256((size_t)batch * sf * sizeof(float2));
+  double2* R = (double2*)w;
+  w += al256((size_t)batch * sr * sizeof(double2));
+  double2* D = nullptr;
+  if (sweeps > 1) {
+    D = (double2*)w;
+    w += al256((size_t)batch * sr * sizeof(double2));
+  }
+  unsigned* nrm = (unsigned*)w;
+  int rc;
+  // FP32 factorisation and first solve on the complex64 copy
+  {
+    dim3 g(ir_grid_x((long long)n * (n + nrhs)), batch);
+    ir_to_f32_kernel<<<g, IR_NT, 0, s>>>(M, ld, stride, Mf, sf, n, n + nrhs);
+    count_launch();
+    RCWA_LAUNCH_CHECK();
+  }
+  if ((rc = lu_factor<float2>(s, n, Mf, n, sf, batch, piv, status))) return rc;
+  if (nrhs <= 0) return RCWA_OK;
+  if ((rc = lu_compose(s, n, piv, batch))) return rc;
+  if ((rc = lu_solve<float2>(s, n, nrhs, Mf, n, sf, batch, piv))) return rc;
+  const dim3 gr(ir_grid_x(sr), batch);
+  float2* Xf = Mf + (long long)n * n;   // right-hand-side part of the complex64 system
+  ir_take_x0_kernel<<<gr, IR_NT, 0, s>>>(M, ld, stride, R, Xf, sf, n, nrhs);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  // R = B - A X0 in FP64 (DMMA); A is the untouched FP64 A part of M
+  auto residual = [&](const double2* X, int ldx, long long sx) {
+    ZGemm gm;
+    gm.m = n;
+    gm.n = nrhs;
+    gm.k = n;
+    gm.alpha = cmk(-1.0, 0.0);
+    gm.beta = cmk(1.0, 0.0);
+    gm.A = M;
+    gm.lda = ld;
+    gm.sA = stride;
+    gm.B = X;
+    gm.ldb = ldx;
+    gm.sB = sx;
+    gm.C = R;
+    gm.ldc = n;
+    gm.sC = sr;
+    gm.batch = batch;
+    return zgemm(s, gm);
+  };
+  if ((rc = residual(M + (long long)n * ld, ld, stride))) return rc;
+  for (int it = 0; it < sweeps; ++it) {
+    const bool last = it + 1 == sweeps;
+    ir_residual_f32_kernel<<<gr, IR_NT, 0, s>>>(R, Xf, sf, n, nrhs);
+    count_launch();
+    RCWA_LAUNCH_CHECK();
+    if ((rc = lu_solve<float2>(s, n, nrhs, Mf, n, sf, batch, piv))) return rc;
+    if (last) RCWA_CUDA_TRY(cudaMemsetAsync(nrm, 0, (size_t)batch * 2 * sizeof(unsigned), s));
+    ir_update_kernel<<<gr, IR_NT, 0, s>>>(M, ld, stride, Xf, sf, last ? nullptr : D, n, nrhs, nrm);
+    count_launch();
+    RCWA_LAUNCH_CHECK();
+    // R <- R - A dX: the residual of the corrected X without a copy of B
+    if (!last && (rc = residual(D, n, sr))) return rc;
+  }
+  ir_flag_kernel<<<cdiv_up(batch, 128), 128, 0, s>>>(nrm, status, batch, 1e-4f);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  return RCWA_OK;
 }
 
 }  // namespace rcwa

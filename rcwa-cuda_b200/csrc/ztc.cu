@@ -50,10 +50,11 @@ __device__ __forceinline__ uint32_t tile_off(int row, int k) {
   return (uint32_t)((k >> 2) * 2048 + (row >> 3) * 128 + (row & 7) * 16 + (k & 3) * 4);
 }
 
+// v = hi + lo + O(2^-22 |v|): hi = tf32(v), lo = tf32(v - hi) with the
+// remainder taken from the double itself
 __device__ __forceinline__ void put_split(uint8_t* hi_tile, uint8_t* lo_tile, int row, int k, double v) {
-  const float f = (float)v;
-  const uint32_t h = to_tf32(f);
-  const uint32_t l = to_tf32(f - __uint_as_float(h));
+  const uint32_t h = to_tf32((float)v);
+  const uint32_t l = to_tf32((float)(v - (double)__uint_as_float(h)));
   const uint32_t o = tile_off(row, k);
   *reinterpret_cast<uint32_t*>(hi_tile + o) = h;
   *reinterpret_cast<uint32_t*>(lo_tile + o) = l;

@@ -1,6 +1,8 @@
 // The reference's built-in case (rcwa3d/src/main.cpp:35-198) written against
 // the rcwa_b200 C++ host API: once step by step with the reference's function
-// names, once as a single GPU solve.  Build: see INTEGRATION.md.
+// names, once as a single GPU solve.  Build from the repository root:
+//   g++ -std=c++17 -O2 -Iinclude -Ircwa-cuda_b200/host rcwa-cuda_b200/host/demo_main.cpp \
+//       -Lrcwa-cuda_b200/rcwa_b200 -lrcwa_b200 -Wl,-rpath,<dir of librcwa_b200.so> -o demo_main
 #include <cmath>
 #include <cstdio>
 #include <vector>

@@ -173,12 +173,12 @@ def c2_sweep(n_lambda: int = 201, grid: int = 256, harmonics: int = 7,
     return Problem(f"c2_sweep_h{harmonics}", st, srcs, ParamSpec(harmonics, harmonics, 1.0, 1.0, 2.25, 1.0))
 
 
-def c3_request(rng: np.random.Generator, grid: int = 256, m_max: int = 21) -> Problem:
-    """One solve of the uneven batch: odd M in 5..m_max (h=(M-1)/2), 1-6 layers
+def c3_request(rng: np.random.Generator, grid: int = 256, m_max: int = 21, m_min: int = 5) -> Problem:
+    """One solve of the uneven batch: odd M in m_min..m_max (h=(M-1)/2), 1-6 layers
     of pillar / hole / line-space, fill U[0.2,0.8], t U[20,300], square period
     U[300,800], lambda U[300,900], theta U[0,60 deg], phi U[0,90 deg],
     eps re U[1.5,16], im U[0,1]; superstrate air, substrate 2.25."""
-    M = int(rng.choice(np.arange(5, m_max + 1, 2)))
+    M = int(rng.choice(np.arange(m_min, m_max + 1, 2)))
     h = (M - 1) // 2
     L = int(rng.integers(1, 7))
     period = float(rng.uniform(300.0, 800.0))

@@ -29,9 +29,16 @@ STATUS_SINGULAR = 1
 STATUS_EIG_NOCONV = 2
 STATUS_NONFINITE = 4
 STATUS_WOOD_ANOMALY = 8
+STATUS_REFINE_SLOW = 16
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+# stages that PREC_MIXED runs in reduced precision (Context.set_mixed)
+MIXED_LAYER_GEMM = 1
+MIXED_STAR_GEMM = 2
+MIXED_LAYER_LU = 4
+MIXED_STAR_LU = 8
+MIXED_ALL = 15
 GEOM_LI_RULE = 1   # rcwa_geometry_create_ex: Li's factorization rule
 
 
@@ -89,6 +96,7 @@ _SIGS = {
     "rcwa_context_set_stream": ([_VP, _VP], C.c_int),
     "rcwa_context_synchronize": ([_VP], C.c_int),
     "rcwa_context_kernel_launches": ([_VP, C.POINTER(C.c_uint64)], C.c_int),
+    "rcwa_context_set_mixed": ([_VP, C.c_uint, C.c_int], C.c_int),
     "rcwa_profile_enable": ([C.c_int], C.c_int),
     "rcwa_profile_reset": ([], C.c_int),
     "rcwa_profile_query": ([C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64),
@@ -117,6 +125,7 @@ _SIGS = {
     "rcwa_eig": ([_VP, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_eig_noalloc": ([C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_lu_solve": ([_VP, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
+    "rcwa_lu_solve_ex": ([_VP, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP, C.c_int, C.c_int], C.c_int),
     "rcwa_gemm_ex": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, CComplex, _VP, _VP,
                       CComplex, _VP], C.c_int),
     "rcwa_gemm": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, C.c_int], C.c_int),
@@ -414,7 +423,12 @@ class Context:
             return lam[0], W[0], int(st[0])
         return lam, W, st
 
-    def lu_solve(self, A, B):
+    def set_mixed(self, stages: int = MIXED_ALL, refine_sweeps: int = 1):
+        """Stages run in reduced precision by PREC_MIXED solves on this context
+        and the FP64 refinement sweeps of their LU solves."""
+        _check(self.lib.rcwa_context_set_mixed(self.h, stages, refine_sweeps))
+
+    def lu_solve(self, A, B, precision: int = PREC_FP64, refine_sweeps: int = 1):
         A = np.asarray(A, dtype=np.complex128)
         B = np.asarray(B, dtype=np.complex128)
         single = A.ndim == 2
@@ -428,8 +442,8 @@ class Context:
         Bf = np.ascontiguousarray(B.transpose(0, 2, 1))
         X = np.zeros((b, m, n), np.complex128)
         st = np.zeros(b, np.uint32)
-        _check(self.lib.rcwa_lu_solve(self.h, n, m, b, _ptr(Af), _ptr(Bf), _ptr(X), _ptr(st)),
-               allow_numeric=True)
+        _check(self.lib.rcwa_lu_solve_ex(self.h, n, m, b, _ptr(Af), _ptr(Bf), _ptr(X), _ptr(st),
+                                         precision, refine_sweeps), allow_numeric=True)
         X = X.transpose(0, 2, 1)
         return (X[0], int(st[0])) if single else (X, st)
 

@@ -69,3 +69,23 @@ def test_eig_noalloc_rejects_oversize():
     assert b"scratch" in lib.rcwa_last_error()
     rc = lib.rcwa_eig_noalloc(128, 64, dummy, dummy, dummy, dummy, None)
     assert rc == L.RCWA_ERR_INVALID
+    # the documented largest batches: one more matrix no longer fits
+    for n, bmax in ((32, 56), (64, 22), (98, 11), (128, 7)):
+        rc = lib.rcwa_eig_noalloc(n, bmax + 1, dummy, dummy, dummy, dummy, None)
+        assert rc == L.RCWA_ERR_INVALID, (n, bmax)
+
+
+def test_eig_noalloc_largest_documented_batch():
+    """n = 128 with the documented largest batch (7) runs and matches rcwa_eig."""
+    torch = pytest.importorskip("torch")
+    from rcwa_b200 import lib as L
+    lib = L.load()
+    ctx = L.Context(0)
+    rng = np.random.default_rng(7)
+    A = rng.standard_normal((7, 128, 128)) + 1j * rng.standard_normal((7, 128, 128))
+    lam_ref, W_ref, st_ref = ctx.eig(A)
+    lam, W, st = _run_noalloc(lib, A, torch)
+    assert not st.any() and not st_ref.any()
+    assert np.abs(lam - lam_ref).max() <= TOL * np.abs(lam_ref).max()
+    assert np.abs(W - W_ref).max() <= TOL
+    ctx.close()
