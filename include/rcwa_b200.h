@@ -54,15 +54,20 @@ extern "C" {
                               precision; FP64 Omega^2, eig, sqrt, exp and efficiency sums */
 
 /* Stages that RCWA_PREC_MIXED runs in reduced precision.  GEMM stages use the
- * split-TF32 tensor-core GEMM (each FP64 operand split into TF32 hi + lo,
- * three tcgen05 kind::tf32 products accumulated in FP32); LU stages factor
- * and solve in FP32 (complex64) and refine the solution with FP64 residuals
+ * int8-sliced tensor-core GEMM (each row of A and column of B scaled by a
+ * power of two and cut into four signed 7-bit digits, digit products
+ * accumulated exactly in int32 by tcgen05 kind::i8, combined in FP64: about
+ * 29 bits of every product), or with RCWA_MIXED_GEMM_TF32 the split-TF32
+ * GEMM (each FP64 operand split into TF32 hi + lo, three tcgen05 kind::tf32
+ * products accumulated in the tensor core's FP32).  LU stages factor and
+ * solve in FP32 (complex64) and refine the solution with FP64 residuals
  * R = B - A X computed on the FP64 tensor cores. */
 #define RCWA_MIXED_LAYER_GEMM 1u  /* V = Q W / lambda and the layer-assembly products (rcwa.cpp:326-348) */
 #define RCWA_MIXED_STAR_GEMM 2u   /* star-product and global-column products (rcwa.cpp:602-611) */
 #define RCWA_MIXED_LAYER_LU 4u    /* W^-1, V^-1, A^-1 and D^-1 solves of a layer (rcwa.cpp:335-348) */
 #define RCWA_MIXED_STAR_LU 8u     /* star-product and global-column solves (rcwa.cpp:605-611) */
 #define RCWA_MIXED_ALL 15u
+#define RCWA_MIXED_GEMM_TF32 16u  /* GEMM stages on split-TF32 instead of int8 slices */
 
 typedef struct rcwa_complex {
   double re, im;
@@ -315,7 +320,9 @@ int rcwa_lu_solve_ex(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_c
                      const rcwa_complex* B, rcwa_complex* X, uint32_t* status, int precision,
                      int refine_sweeps);
 /* C = A * B (m x k times k x n, column-major host arrays), batched; precision
- * selects FP64 or split-TF32 (the Eigen operator* products of rcwa.cpp). */
+ * selects FP64 or the context's mixed-precision GEMM -- int8 slices, or
+ * split-TF32 with RCWA_MIXED_GEMM_TF32 (the Eigen operator* products of
+ * rcwa.cpp). */
 int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_complex* A,
               const rcwa_complex* B, rcwa_complex* C, int precision);
 /* C = alpha op(A) op(B) + beta C, batched, column-major host arrays; op = 1

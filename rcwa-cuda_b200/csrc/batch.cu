@@ -357,8 +357,7 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
     } else {
       for (int l = 0; l < k.nl; ++l) np += k.uniform[l] ? 0 : 1;
     }
-    const size_t per = sweep_bytes_per_source(d, np, active_ir_sweeps(ctx)) +
-                       geometry_bytes_per_item(d, nl, k.nx, k.ny);
+    const size_t per = sweep_bytes_per_source(ctx, d, np) + geometry_bytes_per_item(d, nl, k.nx, k.ny);
     int chunk = (int)std::max<size_t>(1, budget / kmax / per);
     // launch grids index matrices in a 65535-wide grid dimension: at most
     // 2 * layers * items systems per batched LU

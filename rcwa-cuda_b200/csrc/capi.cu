@@ -140,7 +140,8 @@ int rcwa_context_kernel_launches(rcwa_context* c, uint64_t* count) {
 
 int rcwa_context_set_mixed(rcwa_context* c, unsigned stages, int refine_sweeps) {
   CHECK_ARG(c, "NULL context");
-  CHECK_ARG((stages & ~(unsigned)RCWA_MIXED_ALL) == 0, "unknown mixed-precision stage bits");
+  CHECK_ARG((stages & ~(unsigned)(RCWA_MIXED_ALL | RCWA_MIXED_GEMM_TF32)) == 0,
+            "unknown mixed-precision stage bits");
   CHECK_ARG(refine_sweeps >= 1 && refine_sweeps <= 4, "refine_sweeps must be 1..4");
   c->mixed_stages = stages;
   c->ir_sweeps = refine_sweeps;
@@ -523,7 +524,10 @@ int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_comp
   CHECK_ARG(precision == RCWA_PREC_FP64 || precision == RCWA_PREC_MIXED, "unknown precision mode");
   RCWA_CUDA_TRY(cudaSetDevice(ctx->device));
   const size_t na = (size_t)m * k, nb = (size_t)k * n, nc = (size_t)m * n;
-  int rc = ctx_reserve(ctx, (na + nb + nc) * batch * 16 + 1024);
+  const int kind = precision != RCWA_PREC_MIXED ? 0 : (ctx->mixed_stages & RCWA_MIXED_GEMM_TF32) ? TC_TF32 : TC_INT8;
+  const size_t base = ((na + nb + nc) * batch * 16 + 511) & ~(size_t)255;
+  const size_t wsb = kind == TC_INT8 ? zgemm_oz_ws_bytes(m, n, k, batch) : 0;
+  int rc = ctx_reserve(ctx, base + wsb + 1024);
   if (rc) return rc;
   double2* dA = (double2*)ctx->ws;
   double2* dB = dA + na * batch;
@@ -536,7 +540,9 @@ int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_comp
   g.A = dA; g.lda = m; g.sA = (long long)na;
   g.B = dB; g.ldb = k; g.sB = (long long)nb;
   g.C = dC; g.ldc = m; g.sC = (long long)nc;
-  g.tc = precision == RCWA_PREC_MIXED ? 1 : 0;
+  g.tc = kind;
+  g.ws = (char*)ctx->ws + base;
+  g.ws_bytes = wsb;
   int* terr = g.tc ? tc_error_flag() : nullptr;
   if (terr) RCWA_CUDA_TRY(cudaMemsetAsync(terr, 0, sizeof(int), s));
   if ((rc = zgemm(s, g))) return rc;

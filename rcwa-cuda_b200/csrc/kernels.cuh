@@ -37,11 +37,20 @@ struct ZGemm {
   long long sdr = 0;
   int batch = 1;
   int opA = 0, opB = 0;         // 1 = use the conjugate transpose of the stored operand
-  int tc = 0;                   // 1 = split-TF32 on tcgen05 (mixed-precision mode)
+  // reduced-precision kernels of the mixed mode: 0 = FP64, TC_TF32 = split-TF32
+  // on tcgen05 (ztc.cu), TC_INT8 = int8 digit slices on tcgen05 (zoz.cu,
+  // needs ws of zgemm_oz_ws_bytes)
+  int tc = 0;
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
 };
+enum { TC_TF32 = 1, TC_INT8 = 2 };
 int zgemm(cudaStream_t s, const ZGemm& g);
 // split-TF32 tcgen05 GEMM (ztc.cu); *err is set when a bounded wait expires
 int zgemm_tc(cudaStream_t s, const ZGemm& g, int* err);
+// int8-sliced tcgen05 GEMM (zoz.cu); *err is set when a bounded wait expires
+size_t zgemm_oz_ws_bytes(int m, int n, int k, int batch);
+int zgemm_oz(cudaStream_t s, const ZGemm& g, int* err);
 int* tc_error_flag();   // device flag of the current device (set-up once per device)
 
 // X = A^-1 B on the augmented [A | B] (n x (n+nrhs), column-major, ld >= n),

@@ -235,6 +235,24 @@ int active_ir_sweeps(const rcwa_context* ctx) {
   return (ctx->tc & (RCWA_MIXED_LAYER_LU | RCWA_MIXED_STAR_LU)) ? ctx->ir_sweeps : 0;
 }
 
+static bool int8_gemms(const rcwa_context* ctx) {
+  return (ctx->tc & (RCWA_MIXED_LAYER_GEMM | RCWA_MIXED_STAR_GEMM)) && !(ctx->tc & RCWA_MIXED_GEMM_TF32);
+}
+
+void set_gemm_kind(const rcwa_context* ctx, unsigned stage, ZGemm& g) {
+  g.tc = 0;
+  g.ws = nullptr;
+  g.ws_bytes = 0;
+  if (!(ctx->tc & stage)) return;
+  if (ctx->tc & RCWA_MIXED_GEMM_TF32) {
+    g.tc = TC_TF32;
+    return;
+  }
+  g.tc = TC_INT8;
+  g.ws = ctx->ozws;
+  g.ws_bytes = ctx->ozws_bytes;
+}
+
 // One batched solve of the S-matrix algebra: FP64 LU, or -- when `stage` runs
 // mixed in this solve -- FP32 LU with FP64 refinement in the chunk's
 // refinement workspace.
@@ -276,7 +294,7 @@ int star_product(rcwa_context* ctx, int B, int n, SMat& A, const SMat& Bm, doubl
     g.B = Y; g.ldb = n; g.sB = sY;
     g.C = C; g.ldc = n; g.sC = sC;
     g.batch = B;
-    g.tc = (ctx->tc & RCWA_MIXED_STAR_GEMM) ? 1 : 0;
+    set_gemm_kind(ctx, RCWA_MIXED_STAR_GEMM, g);
     return zgemm(s, g);
   };
   const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
@@ -351,7 +369,7 @@ constexpr int kBlocksPerSource = 4 + 1 + 4 + 4 + 2 + 3 + 6;  // SD,tmp,s0-3,augW
 
 // ir > 0: room for the refinement workspace of the largest mixed-precision
 // solve of a chunk (the star product's 2B systems with 2n right-hand sides)
-size_t plan_bytes(const ModeDims& d, int B, int np, int ir = 0) {
+size_t plan_bytes(const ModeDims& d, int B, int np, int ir = 0, bool oz = false) {
   const size_t nn = (size_t)d.n * d.n;
   const int ne = np > 0 ? np : 1;
   size_t b = (size_t)B * kBlocksPerSource * nn * sizeof(double2);
@@ -363,13 +381,15 @@ size_t plan_bytes(const ModeDims& d, int B, int np, int ir = 0) {
   b += (size_t)B * sizeof(SourceDev) + (size_t)3 * B * sizeof(uint32_t);
   b += (size_t)2 * B * d.n * sizeof(int);
   if (ir > 0) b += zgesv_ir_ws_bytes(d.n, 2 * d.n, 2 * B, ir);
+  if (oz) b += zgemm_oz_ws_bytes(d.n, d.n, d.n, B);   // the largest product of a chunk
   b += 64 * 256;  // alignment slack
   return (b + 255) & ~(size_t)255;  // callers place further buffers right after the plan
 }
 
 int plan_take(rcwa_context* ctx, const ModeDims& d, int B, int np, Plan& pl) {
   const int ir = active_ir_sweeps(ctx);
-  int rc = ctx_reserve(ctx, plan_bytes(d, B, np, ir));
+  const bool oz = int8_gemms(ctx);
+  int rc = ctx_reserve(ctx, plan_bytes(d, B, np, ir, oz));
   if (rc) return rc;
   char* w = (char*)ctx->ws;
   auto take = [&](size_t bytes) {
@@ -419,6 +439,12 @@ int plan_take(rcwa_context* ctx, const ModeDims& d, int B, int np, Plan& pl) {
   if (ir > 0) {
     ctx->irws_bytes = zgesv_ir_ws_bytes(d.n, 2 * d.n, 2 * B, ir);
     ctx->irws = take(ctx->irws_bytes);
+  }
+  ctx->ozws = nullptr;
+  ctx->ozws_bytes = 0;
+  if (oz) {
+    ctx->ozws_bytes = zgemm_oz_ws_bytes(d.n, d.n, d.n, B);
+    ctx->ozws = take(ctx->ozws_bytes);
   }
   return RCWA_OK;
 }
@@ -518,7 +544,6 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   const long long nn = (long long)n * n;
   const long long s2 = 2 * nn, s3 = 3 * nn;
   const double2 one = make_double2(1, 0), mone = make_double2(-1, 0), zero = make_double2(0, 0);
-  const int ltc = (ctx->tc & RCWA_MIXED_LAYER_GEMM) ? 1 : 0;
   int rc;
   // Q_i (:280-286) again (P is not needed past Omega^2)
   if ((rc = layer_pq(s, g, l, B, pl))) return rc;
@@ -537,7 +562,7 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   gm.B = pl.augWV; gm.ldb = n; gm.sB = s2;
   gm.C = augV; gm.ldc = n; gm.sC = s2;
   gm.dr = pl.ilam; gm.sdr = n;
-  gm.tc = ltc;
+  set_gemm_kind(ctx, RCWA_MIXED_LAYER_GEMM, gm);
   if ((rc = zgemm(s, gm))) return rc;
   // W^-1, V^-1 (:335-336), one batched solve for both
   if ((rc = set_identity(s, pl.augWV, n, n, s2, 2 * n, n, 2 * B, one))) return rc;
@@ -560,7 +585,7 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   gm.B = Ai; gm.ldb = n; gm.sB = s2;
   gm.C = pl.s2; gm.ldc = n; gm.sC = nn;
   gm.dr = pl.X; gm.sdr = n;
-  gm.tc = ltc;
+  set_gemm_kind(ctx, RCWA_MIXED_LAYER_GEMM, gm);
   if ((rc = zgemm(s, gm))) return rc;
   // D = A - X T1 B -> augD[0] (:346)
   if ((rc = copy_blocks(s, pl.augD, s3, pl.s1, nn, nn, B))) return rc;
@@ -571,14 +596,14 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   gm.B = pl.s0; gm.ldb = n; gm.sB = nn;
   gm.C = pl.augD; gm.ldc = n; gm.sC = s3;
   gm.dl = pl.X; gm.sdl = n;
-  gm.tc = ltc;
+  set_gemm_kind(ctx, RCWA_MIXED_LAYER_GEMM, gm);
   if ((rc = zgemm(s, gm))) return rc;
   // R1 = X T1 A - B -> augD[1] (:347)
   if ((rc = copy_blocks(s, pl.augD + nn, s3, pl.s0, nn, nn, B))) return rc;
   gm.alpha = one; gm.beta = mone;
   gm.B = pl.s1;
   gm.C = pl.augD + nn;
-  gm.tc = ltc;
+  set_gemm_kind(ctx, RCWA_MIXED_LAYER_GEMM, gm);
   if ((rc = zgemm(s, gm))) return rc;
   // T3 = A^-1 B -> s3 ; R2 = A - B T3 -> s1 (in place) (:348)
   gm = ZGemm();
@@ -586,13 +611,13 @@ int patterned_layer(rcwa_context* ctx, const Layers& g, int l, Plan& pl, const d
   gm.A = Ai; gm.lda = n; gm.sA = s2;
   gm.B = pl.s0; gm.ldb = n; gm.sB = nn;
   gm.C = pl.s3; gm.ldc = n; gm.sC = nn;
-  gm.tc = ltc;
+  set_gemm_kind(ctx, RCWA_MIXED_LAYER_GEMM, gm);
   if ((rc = zgemm(s, gm))) return rc;
   gm.alpha = mone; gm.beta = one;
   gm.A = pl.s0; gm.sA = nn;
   gm.B = pl.s3; gm.sB = nn;
   gm.C = pl.s1;
-  gm.tc = ltc;
+  set_gemm_kind(ctx, RCWA_MIXED_LAYER_GEMM, gm);
   if ((rc = zgemm(s, gm))) return rc;
   // X R2 -> augD[2]; then [D | R1 | X R2] -> S11 = D^-1 R1 (:347), S12 = D^-1 X R2 (:348)
   if ((rc = scale_rows(s, pl.s1, n, n, n, nn, pl.X, n, B))) return rc;
@@ -629,7 +654,7 @@ int star_product_bd(rcwa_context* ctx, int B, const ModeDims& d, SMat& A, const 
   if ((rc = lu_stage(ctx, RCWA_MIXED_STAR_LU, n, 2 * n, augFG, n, s3, 2 * B, piv, st))) return rc;
   ZGemm g;
   g.m = n; g.n = n; g.k = n; g.batch = B;
-  g.tc = (ctx->tc & RCWA_MIXED_STAR_GEMM) ? 1 : 0;
+  set_gemm_kind(ctx, RCWA_MIXED_STAR_GEMM, g);
   // S11 = A11 + A12 X1
   g.alpha = one; g.beta = one;
   g.A = A.p[1]; g.lda = n; g.sA = A.s[1];
@@ -680,7 +705,7 @@ int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, c
     g.A = X; g.lda = n; g.sA = sX;
     g.B = Y; g.ldb = n; g.sB = sY;
     g.C = C; g.ldc = n; g.sC = sC;
-    g.tc = (ctx->tc & RCWA_MIXED_STAR_GEMM) ? 1 : 0;
+    set_gemm_kind(ctx, RCWA_MIXED_STAR_GEMM, g);
     return zgemm(s, g);
   };
   // [G1 | R22 D12 | R21 E] in augFG (stride 6n^2)
@@ -721,8 +746,12 @@ int global_columns(rcwa_context* ctx, int B, const ModeDims& d, const SMat& D, c
 
 }  // namespace
 
-size_t sweep_bytes_per_source(const ModeDims& d, int np, int ir_sweeps) {
-  return plan_bytes(d, 1, np, ir_sweeps);
+size_t sweep_bytes_per_source(const ModeDims& d, int np, int ir_sweeps, bool oz) {
+  return plan_bytes(d, 1, np, ir_sweeps, oz);
+}
+
+size_t sweep_bytes_per_source(const rcwa_context* ctx, const ModeDims& d, int np) {
+  return plan_bytes(d, 1, np, active_ir_sweeps(ctx), int8_gemms(ctx));
 }
 
 // The layer set of one geometry, shared by every solve of a sweep.
@@ -913,7 +942,7 @@ int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* s
   }
   int np = 0;
   for (int l = 0; l < g->nl; ++l) np += g->uniform[l] ? 0 : 1;
-  const size_t per = plan_bytes(d, 1, np, active_ir_sweeps(ctx));
+  const size_t per = sweep_bytes_per_source(ctx, d, np);
   int chunk = (int)std::max<size_t>(1, budget / per);
   chunk = std::min(chunk, B);
   const Layers G = layers_of(g);

@@ -30,6 +30,9 @@ struct rcwa_context {
   // refinement workspace of the current sweep chunk (inside ws), see zgesv_ir
   void* irws = nullptr;
   size_t irws_bytes = 0;
+  // int8-slice GEMM workspace of the current sweep chunk (inside ws), see zgemm_oz
+  void* ozws = nullptr;
+  size_t ozws_bytes = 0;
   // worker contexts (own stream + workspace) that run independent group
   // chunks of rcwa_solve_batch concurrently; owned by this context
   std::vector<rcwa_context*> workers;
@@ -123,10 +126,15 @@ int sweep_device(rcwa_context* ctx, const rcwa_geometry* g, const rcwa_source* s
 // Bytes of device workspace per source for a sweep at this size with np
 // patterned layers; ir_sweeps > 0 adds the refinement workspace of the
 // mixed-precision LU stages.
-size_t sweep_bytes_per_source(const ModeDims& d, int np, int ir_sweeps = 0);
+size_t sweep_bytes_per_source(const ModeDims& d, int np, int ir_sweeps = 0, bool oz = false);
+// the same for the mixed-precision stages active in ctx's running solve
+size_t sweep_bytes_per_source(const rcwa_context* ctx, const ModeDims& d, int np);
 // ir_sweeps of a context's running solve: its refinement sweeps when an LU
 // stage runs mixed, else 0.
 int active_ir_sweeps(const rcwa_context* ctx);
+// The GEMM kernel of `stage` in the running solve (0 = FP64, TC_TF32,
+// TC_INT8) with its workspace filled in.
+void set_gemm_kind(const rcwa_context* ctx, unsigned stage, ZGemm& g);
 
 // Dense building blocks on device pointers (used by the step-level ABI).
 struct SMat {

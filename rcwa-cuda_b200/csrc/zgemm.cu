@@ -483,7 +483,7 @@ int zgemm(cudaStream_t s, const ZGemm& g) {
       set_last_error("tensor-core GEMM: device flag unavailable");
       return RCWA_ERR_CUDA;
     }
-    return zgemm_tc(s, g, err);
+    return g.tc == TC_INT8 ? zgemm_oz(s, g, err) : zgemm_tc(s, g, err);
   }
   // k <= 0 gives C = beta*C (the accumulators stay 0)
   dim3 grid(cdiv_up(g.n, BN), cdiv_up(g.m, BM), g.batch);

@@ -1,0 +1,510 @@
+// Complex GEMM on the 5th-generation tensor cores with int8 slices (an
+// Ozaki-style splitting), the GEMM of the mixed-precision solve mode.
+//
+//   C = alpha * diag(dl) * A * B * diag(dr) + beta * C       (complex128 I/O)
+//
+// Why slices: tcgen05 has no FP64 kind, and the FP32 accumulation of its
+// kind::tf32 products does not round like IEEE FP32 -- in the C2 sweep the
+// split-TF32 GEMM (ztc.cu) alone moves R/T by ~8e-6.  Integer products
+// accumulate exactly in int32, so the only error left is the truncation of
+// the operands to a fixed number of 7-bit digits.
+//
+// Splitting (one pass per operand, oz_split_a / oz_split_b): every row i of A
+// gets a power-of-two scale sigma_i > 2 max_j max(|Re a_ij|, |Im a_ij|), so
+// that r = a / sigma_i has |r| < 1/2 in both parts; S signed digits follow
+// from d_s = rint(128 r_{s-1}), r_s = 128 r_{s-1} - d_s, |d_s| <= 64 (exact in
+// FP64), i.e. a = sigma_i sum_s d_s 2^(-7 s) + O(sigma_i 2^(-7 S - 1)).
+// Columns of B get tau_j the same way.  The digit planes are written in the
+// tcgen05 shared-memory image (K-major, no swizzle: 8-row x 16-byte core
+// matrices), one 128-row x 32-k block of A (4096 bytes per plane) or TN-column
+// x 32-k block of B after another, so that the GEMM moves each k-step's
+// operands with two bulk copies.  A gets the planes Re, Im and -Im per digit
+// (integer MMAs have no negate bit), B the planes Re and Im.
+//
+// Products: digit pairs (s, t) with s + t <= S - 1 (0-based) are kept --
+// S (S + 1) / 2 pairs, each four real int8 MMAs:
+//   Re C_g += Re A_s Re B_t + (-Im A_s) Im B_t,  Im C_g += Re A_s Im B_t + Im A_s Re B_t
+// into int32 accumulators in tensor memory, one per g = s + t and part
+// (2 S accumulators of TN columns).  |products| <= 4096, so up to
+// 2^31 / (8 S 4096) > 16000 k-values accumulate without overflow.  The
+// epilogue forms sum_g acc_g 2^(-7 (g + 2)) exactly in FP64 and scales by
+// sigma_i tau_j.  Error ~ 2^(-7 S) sigma_i tau_j sqrt(k): S = 4 keeps ~29 bits
+// of every product of the two operands' row / column maxima.
+//
+// Pipeline (per CTA, 128 threads, 128 x TN complex tile): thread 0 issues the
+// bulk copies (cp.async.bulk with mbarrier complete_tx) of ST stages ahead and
+// the MMAs of each k-step, committing each stage's MMAs to its "empty"
+// mbarrier before the stage is refilled; all four warps then read the
+// accumulators out of tensor memory (tcgen05.ld, warp w owns lanes 32w..32w+31)
+// for the epilogue.  Every mbarrier wait is bounded; on time-out the CTA
+// sets the error flag, waits (bounded) for its own copies and MMAs, frees its
+// tensor memory and returns without writing C.
+#include <cstdint>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace rcwa {
+
+namespace {
+
+constexpr int OZ_NT = 128;              // threads per CTA
+constexpr int OZ_TM = 128;              // complex rows per CTA tile (= MMA M)
+constexpr int OZ_TK = 32;               // k per step (= int8 MMA K)
+constexpr int OZ_APL = OZ_TM * OZ_TK;   // bytes of one A digit plane block
+constexpr long long OZ_WAIT_CAP = 1LL << 26;
+
+template <int TN>
+constexpr int oz_bpl() { return TN * OZ_TK; }   // bytes of one B digit plane block
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// byte offset of (row, k) in a rows x 32 int8 K-major block: 16-byte chunks
+// along k are rows * 16 bytes apart, 8-row groups 128 bytes apart
+__device__ __forceinline__ uint32_t blk_off(int rows, int row, int k) {
+  return (uint32_t)((k >> 4) * (rows * 16) + (row >> 3) * 128 + (row & 7) * 16 + (k & 15));
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);        // start address
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;    // leading byte offset: next 16 bytes along k
+  d |= (uint64_t)((128u >> 4) & 0x3FFF) << 32;   // stride byte offset: next 8-row group
+  d |= (uint64_t)1 << 46;                        // descriptor version (sm_100)
+  return d;                                      // base offset 0, no swizzle
+}
+
+// kind::i8: D s32, A and B signed 8-bit, both K-major, M = 128, N = TN
+template <int TN>
+constexpr uint32_t oz_idesc() {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(OZ_TM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                       uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(bar)));
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+  for (long long it = 0; it < OZ_WAIT_CAP; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(su32(bar)), "r"(phase)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_load(void* sdst, const void* gsrc, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          su32(sdst)),
+      "l"(gsrc), "r"(bytes), "r"(su32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"(bytes) : "memory");
+}
+
+// S signed 7-bit digits of v / sc (|v / sc| < 1/2), most significant first
+template <int S>
+__device__ __forceinline__ void digits(double v, double inv_sc, int (&d)[S]) {
+  double r = v * inv_sc;   // exact: inv_sc is a power of two
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const double t = r * 128.0;
+    const double q = rint(t);
+    d[s] = (int)q;
+    r = t - q;
+  }
+}
+
+// sigma = 2^(e + 1) for max = f 2^e (f in [0.5, 1)): |x| / sigma < 1/2;
+// 1 for an all-zero line, NaN for a line holding a NaN or an infinity (the
+// NaN then reaches every output of the line, as an FP64 product would)
+__device__ __forceinline__ double line_scale(double mx) {
+  if (!(mx <= 1.7976931348623157e308)) return __longlong_as_double(0x7ff8000000000000LL);
+  if (mx == 0.0) return 1.0;
+  int e;
+  frexp(mx, &e);
+  return ldexp(1.0, e + 1);
+}
+
+// A (m x k, column-major, batch stride sA) -> digit planes [b][mb][kb][3S]
+// blocks of 4096 bytes and sigma[b][MB * 128].  One thread per row: the
+// row maximum, then 16 k-values at a time into one 16-byte chunk per plane
+// (consecutive threads write consecutive chunks of a core matrix).
+template <int S>
+__global__ void __launch_bounds__(OZ_TM)
+oz_split_a(const double2* __restrict__ A, int lda, long long sA, int m, int k, int MB, int KB,
+           uint8_t* __restrict__ Aq, double* __restrict__ sig) {
+  const int b = blockIdx.y, mb = blockIdx.x, r = threadIdx.x;
+  const int i = mb * OZ_TM + r;
+  const double2* Ab = A + (long long)b * sA;
+  double mx = 0.0;
+  bool bad = false;
+  if (i < m)
+    for (int kk = 0; kk < k; ++kk) {
+      const double2 v = Ab[(long long)kk * lda + i];
+      mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+      bad = bad || v.x != v.x || v.y != v.y;
+    }
+  const double sc = line_scale(bad ? __longlong_as_double(0x7ff8000000000000LL) : mx);
+  sig[(long long)b * MB * OZ_TM + i] = sc;
+  const bool live = i < m && sc == sc;
+  const double inv = live ? 1.0 / sc : 0.0;
+  uint8_t* base = Aq + ((long long)b * MB + mb) * KB * (3LL * S * OZ_APL);
+  for (int c = 0; c < 2 * KB; ++c) {    // 16-k chunk c of the row
+    uint32_t wr[S][4], wi[S][4], wn[S][4];
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+      for (int w = 0; w < 4; ++w) wr[s][w] = wi[s][w] = wn[s][w] = 0u;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int kk = c * 16 + q;
+      double2 v = make_double2(0.0, 0.0);
+      if (live && kk < k) v = Ab[(long long)kk * lda + i];
+      int dr[S], di[S];
+      digits<S>(v.x, inv, dr);
+      digits<S>(v.y, inv, di);
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const int sh = (q & 3) * 8;
+        wr[s][q >> 2] |= ((uint32_t)(dr[s] & 0xff)) << sh;
+        wi[s][q >> 2] |= ((uint32_t)(di[s] & 0xff)) << sh;
+        wn[s][q >> 2] |= ((uint32_t)((-di[s]) & 0xff)) << sh;
+      }
+    }
+    uint8_t* blk = base + (long long)(c >> 1) * (3LL * S * OZ_APL);
+    const uint32_t off = blk_off(OZ_TM, r, (c & 1) * 16);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      *reinterpret_cast<uint4*>(blk + (3 * s + 0) * OZ_APL + off) = make_uint4(wr[s][0], wr[s][1], wr[s][2], wr[s][3]);
+      *reinterpret_cast<uint4*>(blk + (3 * s + 1) * OZ_APL + off) = make_uint4(wi[s][0], wi[s][1], wi[s][2], wi[s][3]);
+      *reinterpret_cast<uint4*>(blk + (3 * s + 2) * OZ_APL + off) = make_uint4(wn[s][0], wn[s][1], wn[s][2], wn[s][3]);
+    }
+  }
+}
+
+// B (k x n, column-major) -> digit planes [b][nb][kb][2S] blocks of TN * 32
+// bytes and tau[b][NB * TN].  One warp per column (columns are contiguous
+// in k): a shuffle-reduced maximum, then lane l takes the 16-k chunks
+// l, l + 32, ...
+template <int S, int TN>
+__global__ void __launch_bounds__(256)
+oz_split_b(const double2* __restrict__ B, int ldb, long long sB, int k, int n, int NB, int KB,
+           uint8_t* __restrict__ Bq, double* __restrict__ tau) {
+  constexpr int BPL = oz_bpl<TN>();
+  const int b = blockIdx.y, lane = threadIdx.x & 31;
+  const int j = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (j >= NB * TN) return;   // warp-uniform
+  const double2* col = B + (long long)b * sB + (long long)j * ldb;
+  double mx = 0.0;
+  bool bad = false;
+  if (j < n)
+    for (int kk = lane; kk < k; kk += 32) {
+      const double2 v = col[kk];
+      mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+      bad = bad || v.x != v.x || v.y != v.y;
+    }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  bad = __any_sync(0xffffffffu, bad);
+  const double sc = line_scale(bad ? __longlong_as_double(0x7ff8000000000000LL) : mx);
+  if (lane == 0) tau[(long long)b * NB * TN + j] = sc;
+  const bool live = j < n && sc == sc;
+  const double inv = live ? 1.0 / sc : 0.0;
+  const int nb = j / TN, jr = j % TN;
+  uint8_t* base = Bq + ((long long)b * NB + nb) * KB * (2LL * S * BPL);
+  for (int c = lane; c < 2 * KB; c += 32) {
+    uint32_t wr[S][4], wi[S][4];
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+      for (int w = 0; w < 4; ++w) wr[s][w] = wi[s][w] = 0u;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int kk = c * 16 + q;
+      double2 v = make_double2(0.0, 0.0);
+      if (live && kk < k) v = col[kk];
+      int dr[S], di[S];
+      digits<S>(v.x, inv, dr);
+      digits<S>(v.y, inv, di);
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const int sh = (q & 3) * 8;
+        wr[s][q >> 2] |= ((uint32_t)(dr[s] & 0xff)) << sh;
+        wi[s][q >> 2] |= ((uint32_t)(di[s] & 0xff)) << sh;
+      }
+    }
+    uint8_t* blk = base + (long long)(c >> 1) * (2LL * S * BPL);
+    const uint32_t off = blk_off(TN, jr, (c & 1) * 16);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      *reinterpret_cast<uint4*>(blk + (2 * s + 0) * BPL + off) = make_uint4(wr[s][0], wr[s][1], wr[s][2], wr[s][3]);
+      *reinterpret_cast<uint4*>(blk + (2 * s + 1) * BPL + off) = make_uint4(wi[s][0], wi[s][1], wi[s][2], wi[s][3]);
+    }
+  }
+}
+
+template <int S, int TN>
+struct OzCfg {
+  static constexpr int BPL = oz_bpl<TN>();
+  static constexpr int A_STAGE = 3 * S * OZ_APL;
+  static constexpr int B_STAGE = 2 * S * BPL;
+  static constexpr int STAGE = A_STAGE + B_STAGE;
+  static constexpr int ST = (3 * STAGE <= 200 * 1024) ? 3 : 2;
+  static constexpr int SMEM = ST * STAGE + 1024;        // + 1 KB alignment slack
+  static constexpr uint32_t TMEM_COLS = 512;            // 2 S TN <= 512
+  static_assert(2 * S * TN <= 512, "accumulators exceed tensor memory");
+};
+
+template <int S, int TN>
+__global__ void __launch_bounds__(OZ_NT, 1)
+oz_gemm_kernel(int m, int n, int k, int MB, int NB, int KB, double2 alpha, const uint8_t* __restrict__ Aq,
+               const double* __restrict__ sig, const uint8_t* __restrict__ Bq, const double* __restrict__ tau,
+               double2 beta, double2* __restrict__ C, int ldc, long long sC, const double2* __restrict__ dl,
+               long long sdl, const double2* __restrict__ dr, long long sdr, int* __restrict__ err) {
+  using Cfg = OzCfg<S, TN>;
+  constexpr int ST = Cfg::ST;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full[ST], empty[ST], done;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int s_ok;
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int bz = blockIdx.z, mb = blockIdx.y, nb = blockIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint8_t* Ab = Aq + ((long long)bz * MB + mb) * KB * (long long)Cfg::A_STAGE;
+  const uint8_t* Bb = Bq + ((long long)bz * NB + nb) * KB * (long long)Cfg::B_STAGE;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_slot)),
+                 "r"(Cfg::TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int st = 0; st < ST; ++st) {
+      mbar_init(&full[st]);
+      mbar_init(&empty[st]);
+    }
+    mbar_init(&done);
+    s_ok = 1;
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_slot;
+
+  if (tid == 0) {
+    bool ok = true;
+    int issued = 0;      // k-steps whose operands were requested
+    int committed = 0;   // k-steps whose MMAs were committed
+    auto load = [&](int kt) {
+      const int st = kt % ST;
+      uint8_t* sa = smem + st * Cfg::STAGE;
+      expect_tx(&full[st], (uint32_t)Cfg::STAGE);
+      bulk_load(sa, Ab + (long long)kt * Cfg::A_STAGE, (uint32_t)Cfg::A_STAGE, &full[st]);
+      bulk_load(sa + Cfg::A_STAGE, Bb + (long long)kt * Cfg::B_STAGE, (uint32_t)Cfg::B_STAGE, &full[st]);
+      ++issued;
+    };
+    for (int p = 0; p < ST && p < KB; ++p) load(p);
+    constexpr uint32_t IDESC = oz_idesc<TN>();
+    for (int kt = 0; kt < KB && ok; ++kt) {
+      const int st = kt % ST;
+      // refill the stage that k-step kt-1 used, once its MMAs are done
+      if (kt >= 1 && kt - 1 + ST < KB) {
+        const int ps = (kt - 1) % ST;
+        if (!mbar_wait(&empty[ps], (uint32_t)(((kt - 1) / ST) & 1))) { ok = false; break; }
+        load(kt - 1 + ST);
+      }
+      if (!mbar_wait(&full[st], (uint32_t)((kt / ST) & 1))) { ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t sa = su32(smem + st * Cfg::STAGE), sb = sa + Cfg::A_STAGE;
+#pragma unroll
+      for (int s = 0; s < S; ++s)
+#pragma unroll
+        for (int t = 0; t + s < S; ++t) {
+          const int g = s + t;
+          const uint32_t accr = tmem + (uint32_t)((2 * g) * TN), acci = accr + TN;
+          // the first product into each accumulator overwrites it
+          const uint32_t first = (kt == 0 && s == 0) ? 0u : 1u;
+          const uint64_t dar = smem_desc(sa + (3 * s + 0) * OZ_APL, OZ_TM * 16);
+          const uint64_t dai = smem_desc(sa + (3 * s + 1) * OZ_APL, OZ_TM * 16);
+          const uint64_t dan = smem_desc(sa + (3 * s + 2) * OZ_APL, OZ_TM * 16);
+          const uint64_t dbr = smem_desc(sb + (2 * t + 0) * Cfg::BPL, TN * 16);
+          const uint64_t dbi = smem_desc(sb + (2 * t + 1) * Cfg::BPL, TN * 16);
+          mma_i8(accr, dar, dbr, IDESC, first);
+          mma_i8(accr, dan, dbi, IDESC, 1u);
+          mma_i8(acci, dar, dbi, IDESC, first);
+          mma_i8(acci, dai, dbr, IDESC, 1u);
+        }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          su32(&empty[st])));
+      ++committed;
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(&done)));
+    if (!ok) {
+      // wait (bounded) for the copies still in flight before the CTA exits
+      for (int kt = committed; kt < issued; ++kt) mbar_wait(&full[kt % ST], (uint32_t)((kt / ST) & 1));
+      s_ok = 0;
+    }
+  }
+  __syncthreads();
+  // every MMA committed before `done` has completed once it flips
+  bool ok = mbar_wait(&done, 0u) && s_ok;
+  ok = __syncthreads_and(ok);
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (ok) {
+    const int row = warp * 32 + lane, gi = mb * OZ_TM + row;
+    const double sg = sig[(long long)bz * MB * OZ_TM + gi];
+    const double* tb = tau + (long long)bz * NB * TN + (long long)nb * TN;
+    const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
+    const double2 sl = (dl && gi < m) ? dl[(long long)bz * sdl + gi] : make_double2(1.0, 0.0);
+    for (int c0 = 0; c0 < TN; c0 += 16) {
+      double vr[16], vi[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) vr[q] = vi[q] = 0.0;
+#pragma unroll
+      for (int g = 0; g < S; ++g) {
+        uint32_t ar[16], ai[16];
+        const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(2 * g * TN + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+            "%12, %13, %14, %15}, [%16];\n"
+            : "=r"(ar[0]), "=r"(ar[1]), "=r"(ar[2]), "=r"(ar[3]), "=r"(ar[4]), "=r"(ar[5]), "=r"(ar[6]),
+              "=r"(ar[7]), "=r"(ar[8]), "=r"(ar[9]), "=r"(ar[10]), "=r"(ar[11]), "=r"(ar[12]), "=r"(ar[13]),
+              "=r"(ar[14]), "=r"(ar[15])
+            : "r"(ta));
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+            "%12, %13, %14, %15}, [%16];\n"
+            : "=r"(ai[0]), "=r"(ai[1]), "=r"(ai[2]), "=r"(ai[3]), "=r"(ai[4]), "=r"(ai[5]), "=r"(ai[6]),
+              "=r"(ai[7]), "=r"(ai[8]), "=r"(ai[9]), "=r"(ai[10]), "=r"(ai[11]), "=r"(ai[12]), "=r"(ai[13]),
+              "=r"(ai[14]), "=r"(ai[15])
+            : "r"(ta + (uint32_t)TN));
+        asm volatile("tcgen05.wait::ld.sync.aligned;");
+        const double w = ldexp(1.0, -7 * (g + 2));
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          vr[q] = fma((double)(int)ar[q], w, vr[q]);
+          vi[q] = fma((double)(int)ai[q], w, vi[q]);
+        }
+      }
+      if (gi < m) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int gj = nb * TN + c0 + q;
+          if (gj >= n) continue;
+          const double st_ = sg * tb[c0 + q];
+          double2 v = cmul(alpha, make_double2(vr[q] * st_, vi[q] * st_));
+          if (dl) v = cmul(sl, v);
+          if (dr) v = cmul(v, dr[(long long)bz * sdr + gj]);
+          double2* cp = C + (long long)bz * sC + (long long)gj * ldc + gi;
+          if (use_beta) v = cadd(v, cmul(beta, *cp));
+          *cp = v;
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicOr(err, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS));
+}
+
+constexpr int OZ_S = 4, OZ_TN = 64;
+using OzDefault = OzCfg<OZ_S, OZ_TN>;
+
+size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+struct OzDims {
+  int MB, NB, KB;
+  size_t a_bytes, b_bytes, sig_bytes, tau_bytes;
+};
+OzDims oz_dims(int m, int n, int k, int batch) {
+  OzDims d;
+  d.MB = (m + OZ_TM - 1) / OZ_TM;
+  d.NB = (n + OZ_TN - 1) / OZ_TN;
+  d.KB = (k + OZ_TK - 1) / OZ_TK;
+  d.a_bytes = al256((size_t)batch * d.MB * d.KB * OzDefault::A_STAGE);
+  d.b_bytes = al256((size_t)batch * d.NB * d.KB * OzDefault::B_STAGE);
+  d.sig_bytes = al256((size_t)batch * d.MB * OZ_TM * sizeof(double));
+  d.tau_bytes = al256((size_t)batch * d.NB * OZ_TN * sizeof(double));
+  return d;
+}
+
+}  // namespace
+
+size_t zgemm_oz_ws_bytes(int m, int n, int k, int batch) {
+  if (m <= 0 || n <= 0 || batch <= 0) return 0;
+  const OzDims d = oz_dims(m, n, k < 1 ? 1 : k, batch);
+  return d.a_bytes + d.b_bytes + d.sig_bytes + d.tau_bytes + 256;
+}
+
+int zgemm_oz(cudaStream_t s, const ZGemm& g, int* err) {
+  if (g.m <= 0 || g.n <= 0 || g.batch <= 0) return RCWA_OK;
+  if (g.opA || g.opB) {
+    set_last_error("zgemm_oz: transposed operands are not supported");
+    return RCWA_ERR_INVALID;
+  }
+  const int k = g.k < 1 ? 1 : g.k;   // k <= 0: one zero k-step gives C = beta C
+  const OzDims d = oz_dims(g.m, g.n, k, g.batch);
+  const size_t need = zgemm_oz_ws_bytes(g.m, g.n, k, g.batch);
+  if (!g.ws || g.ws_bytes < need) {
+    set_last_error("zgemm_oz: workspace of %zu bytes, %zu needed", g.ws_bytes, need);
+    return RCWA_ERR_INVALID;
+  }
+  if (g.batch > 65535) {
+    set_last_error("zgemm_oz: batch %d exceeds the grid limit", g.batch);
+    return RCWA_ERR_INVALID;
+  }
+  uint8_t* w = (uint8_t*)(((uintptr_t)g.ws + 255) & ~(uintptr_t)255);
+  uint8_t* Aq = w;
+  uint8_t* Bq = Aq + d.a_bytes;
+  double* sig = (double*)(Bq + d.b_bytes);
+  double* tau = (double*)((uint8_t*)sig + d.sig_bytes);
+  static bool attr[64] = {};   // the attribute is per device
+  int dev = 0;
+  RCWA_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 64 || !attr[dev]) {
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<OZ_S, OZ_TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       OzDefault::SMEM));
+    if (dev < 64) attr[dev] = true;
+  }
+  const int kk = g.k < 0 ? 0 : g.k;
+  void* tok = prof_begin(s);
+  oz_split_a<OZ_S><<<dim3(d.MB, g.batch), OZ_TM, 0, s>>>(g.A, g.lda, g.sA, g.m, kk, d.MB, d.KB, Aq, sig);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  oz_split_b<OZ_S, OZ_TN><<<dim3(cdiv_up((long long)d.NB * OZ_TN, 8), g.batch), 256, 0, s>>>(
+      g.B, g.ldb, g.sB, kk, g.n, d.NB, d.KB, Bq, tau);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  prof_end(s, tok, "zgemm_oz_split");
+  tok = prof_begin(s);
+  oz_gemm_kernel<OZ_S, OZ_TN><<<dim3(d.NB, d.MB, g.batch), OZ_NT, OzDefault::SMEM, s>>>(
+      g.m, g.n, kk, d.MB, d.NB, d.KB, g.alpha, Aq, sig, Bq, tau, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, g.dr,
+      g.sdr, err);
+  prof_end(s, tok, "zgemm_oz");
+  if (tok) prof_add_flops("zgemm_oz", 8.0 * g.m * (double)g.n * (double)kk * g.batch);
+  count_launch();
+  RCWA_LAUNCH_CHECK();
+  return RCWA_OK;
+}
+
+}  // namespace rcwa

@@ -39,6 +39,7 @@ MIXED_STAR_GEMM = 2
 MIXED_LAYER_LU = 4
 MIXED_STAR_LU = 8
 MIXED_ALL = 15
+MIXED_GEMM_TF32 = 16   # GEMM stages on split-TF32 instead of int8 slices
 GEOM_LI_RULE = 1   # rcwa_geometry_create_ex: Li's factorization rule
 
 
