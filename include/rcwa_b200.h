@@ -68,6 +68,7 @@ extern "C" {
 #define RCWA_MIXED_STAR_LU 8u     /* star-product and global-column solves (rcwa.cpp:605-611) */
 #define RCWA_MIXED_ALL 15u
 #define RCWA_MIXED_GEMM_TF32 16u  /* GEMM stages on split-TF32 instead of int8 slices */
+#define RCWA_MIXED_REFINE_INT8 32u  /* LU refinement residuals on the int8-slice GEMM instead of FP64 */
 
 typedef struct rcwa_complex {
   double re, im;
@@ -141,9 +142,11 @@ int rcwa_context_kernel_launches(rcwa_context* ctx, uint64_t* count);
 /* Mixed-precision set-up of this context (no reference counterpart: the
  * reference is FP64 only): the RCWA_MIXED_* stages that RCWA_PREC_MIXED runs
  * in reduced precision (default RCWA_MIXED_ALL; 0 makes RCWA_PREC_MIXED an
- * FP64 solve) and the FP64 refinement sweeps of its LU solves (1..4,
- * default 1).  Sweeps and batches run through the context use it. */
-int rcwa_context_set_mixed(rcwa_context* ctx, unsigned stages, int refine_sweeps);
+ * FP64 solve), the FP64 refinement sweeps of its LU solves (1..4, default 1)
+ * and the 7-bit digits per operand of the int8-slice GEMM (4, 5 or 6,
+ * default 5: about 29, 36 or 43 bits of each product).  Sweeps and batches
+ * run through the context use it. */
+int rcwa_context_set_mixed(rcwa_context* ctx, unsigned stages, int refine_sweeps, int gemm_digits);
 
 /* ---- instrumentation (no reference counterpart: the reference only prints
  * to stdout, rcwa.cpp:92-156).  When enabled, the hot kernel families

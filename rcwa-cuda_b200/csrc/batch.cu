@@ -408,6 +408,7 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
         wc->tc = ctx->tc;
         wc->mixed_stages = ctx->mixed_stages;
         wc->ir_sweeps = ctx->ir_sweeps;
+        wc->oz_digits = ctx->oz_digits;
         cudaError_t e = cudaSetDevice(wc->device);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(wc->stream, start, 0);
         cudaGetLastError();   // launch checks below must see only their own launches

@@ -138,13 +138,15 @@ int rcwa_context_kernel_launches(rcwa_context* c, uint64_t* count) {
   return RCWA_OK;
 }
 
-int rcwa_context_set_mixed(rcwa_context* c, unsigned stages, int refine_sweeps) {
+int rcwa_context_set_mixed(rcwa_context* c, unsigned stages, int refine_sweeps, int gemm_digits) {
   CHECK_ARG(c, "NULL context");
-  CHECK_ARG((stages & ~(unsigned)(RCWA_MIXED_ALL | RCWA_MIXED_GEMM_TF32)) == 0,
+  CHECK_ARG(gemm_digits >= 4 && gemm_digits <= 6, "gemm_digits must be 4, 5 or 6");
+  CHECK_ARG((stages & ~(unsigned)(RCWA_MIXED_ALL | RCWA_MIXED_GEMM_TF32 | RCWA_MIXED_REFINE_INT8)) == 0,
             "unknown mixed-precision stage bits");
   CHECK_ARG(refine_sweeps >= 1 && refine_sweeps <= 4, "refine_sweeps must be 1..4");
   c->mixed_stages = stages;
   c->ir_sweeps = refine_sweeps;
+  c->oz_digits = gemm_digits;
   return RCWA_OK;
 }
 
@@ -526,7 +528,7 @@ int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_comp
   const size_t na = (size_t)m * k, nb = (size_t)k * n, nc = (size_t)m * n;
   const int kind = precision != RCWA_PREC_MIXED ? 0 : (ctx->mixed_stages & RCWA_MIXED_GEMM_TF32) ? TC_TF32 : TC_INT8;
   const size_t base = ((na + nb + nc) * batch * 16 + 511) & ~(size_t)255;
-  const size_t wsb = kind == TC_INT8 ? zgemm_oz_ws_bytes(m, n, k, batch) : 0;
+  const size_t wsb = kind == TC_INT8 ? zgemm_oz_ws_bytes(m, n, k, batch, ctx->oz_digits) : 0;
   int rc = ctx_reserve(ctx, base + wsb + 1024);
   if (rc) return rc;
   double2* dA = (double2*)ctx->ws;
@@ -541,6 +543,7 @@ int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_comp
   g.B = dB; g.ldb = k; g.sB = (long long)nb;
   g.C = dC; g.ldc = m; g.sC = (long long)nc;
   g.tc = kind;
+  g.digits = ctx->oz_digits;
   g.ws = (char*)ctx->ws + base;
   g.ws_bytes = wsb;
   int* terr = g.tc ? tc_error_flag() : nullptr;

@@ -41,6 +41,7 @@ struct ZGemm {
   // on tcgen05 (ztc.cu), TC_INT8 = int8 digit slices on tcgen05 (zoz.cu,
   // needs ws of zgemm_oz_ws_bytes)
   int tc = 0;
+  int digits = 5;               // TC_INT8: 7-bit digits per operand (4, 5 or 6)
   void* ws = nullptr;
   size_t ws_bytes = 0;
 };
@@ -49,7 +50,7 @@ int zgemm(cudaStream_t s, const ZGemm& g);
 // split-TF32 tcgen05 GEMM (ztc.cu); *err is set when a bounded wait expires
 int zgemm_tc(cudaStream_t s, const ZGemm& g, int* err);
 // int8-sliced tcgen05 GEMM (zoz.cu); *err is set when a bounded wait expires
-size_t zgemm_oz_ws_bytes(int m, int n, int k, int batch);
+size_t zgemm_oz_ws_bytes(int m, int n, int k, int batch, int digits);
 int zgemm_oz(cudaStream_t s, const ZGemm& g, int* err);
 int* tc_error_flag();   // device flag of the current device (set-up once per device)
 
@@ -60,9 +61,10 @@ int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride,
 // The same solve by an FP32 (complex64) LU with `sweeps` FP64 residual
 // refinement sweeps (mixed-precision mode); the A part is left unchanged.
 // ws: zgesv_ir_ws_bytes(n, nrhs, batch, sweeps) bytes of device memory.
-size_t zgesv_ir_ws_bytes(int n, int nrhs, int batch, int sweeps);
+// resid_int8 != 0 computes the residuals on the int8-slice GEMM instead.
+size_t zgesv_ir_ws_bytes(int n, int nrhs, int batch, int sweeps, int resid_int8 = 0);
 int zgesv_ir(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch,
-             int* piv, uint32_t* status, void* ws, int sweeps);
+             int* piv, uint32_t* status, void* ws, int sweeps, int resid_int8 = 0);
 
 // Blocked Hessenberg reduction of packed A (zero below the subdiagonal on
 // return) and Z = Q; V is an n x n scratch per matrix, ws hess_ws_bytes().

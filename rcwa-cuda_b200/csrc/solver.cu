@@ -249,6 +249,7 @@ void set_gemm_kind(const rcwa_context* ctx, unsigned stage, ZGemm& g) {
     return;
   }
   g.tc = TC_INT8;
+  g.digits = ctx->oz_digits;
   g.ws = ctx->ozws;
   g.ws_bytes = ctx->ozws_bytes;
 }
@@ -259,12 +260,13 @@ void set_gemm_kind(const rcwa_context* ctx, unsigned stage, ZGemm& g) {
 static int lu_stage(rcwa_context* ctx, unsigned stage, int n, int nrhs, double2* M, int ld,
                     long long stride, int batch, int* piv, uint32_t* status) {
   if (!(ctx->tc & stage)) return zgesv(ctx->stream, n, nrhs, M, ld, stride, batch, piv, status);
-  const size_t need = zgesv_ir_ws_bytes(n, nrhs, batch, ctx->ir_sweeps);
+  const int r8 = (ctx->tc & RCWA_MIXED_REFINE_INT8) ? 1 : 0;
+  const size_t need = zgesv_ir_ws_bytes(n, nrhs, batch, ctx->ir_sweeps, r8);
   if (!ctx->irws || need > ctx->irws_bytes) {
     set_last_error("internal: refinement workspace of %zu bytes, %zu needed", ctx->irws_bytes, need);
     return RCWA_ERR_INVALID;
   }
-  return zgesv_ir(ctx->stream, n, nrhs, M, ld, stride, batch, piv, status, ctx->irws, ctx->ir_sweeps);
+  return zgesv_ir(ctx->stream, n, nrhs, M, ld, stride, batch, piv, status, ctx->irws, ctx->ir_sweeps, r8);
 }
 
 // ---------------------------------------------------------------------------
@@ -380,8 +382,8 @@ size_t plan_bytes(const ModeDims& d, int B, int np, int ir = 0, bool oz = false)
   b += (size_t)B * (4 * d.N + 4 * d.N + 4) * sizeof(double2); // Kx Ky Kzr Kzt, V0, kinc
   b += (size_t)B * sizeof(SourceDev) + (size_t)3 * B * sizeof(uint32_t);
   b += (size_t)2 * B * d.n * sizeof(int);
-  if (ir > 0) b += zgesv_ir_ws_bytes(d.n, 2 * d.n, 2 * B, ir);
-  if (oz) b += zgemm_oz_ws_bytes(d.n, d.n, d.n, B);   // the largest product of a chunk
+  if (ir > 0) b += zgesv_ir_ws_bytes(d.n, 2 * d.n, 2 * B, ir, 1);
+  if (oz) b += zgemm_oz_ws_bytes(d.n, d.n, d.n, B, 6);   // the largest product of a chunk, any digit count
   b += 64 * 256;  // alignment slack
   return (b + 255) & ~(size_t)255;  // callers place further buffers right after the plan
 }
@@ -437,13 +439,13 @@ int plan_take(rcwa_context* ctx, const ModeDims& d, int B, int np, Plan& pl) {
   ctx->irws = nullptr;
   ctx->irws_bytes = 0;
   if (ir > 0) {
-    ctx->irws_bytes = zgesv_ir_ws_bytes(d.n, 2 * d.n, 2 * B, ir);
+    ctx->irws_bytes = zgesv_ir_ws_bytes(d.n, 2 * d.n, 2 * B, ir, 1);
     ctx->irws = take(ctx->irws_bytes);
   }
   ctx->ozws = nullptr;
   ctx->ozws_bytes = 0;
   if (oz) {
-    ctx->ozws_bytes = zgemm_oz_ws_bytes(d.n, d.n, d.n, B);
+    ctx->ozws_bytes = zgemm_oz_ws_bytes(d.n, d.n, d.n, B, 6);
     ctx->ozws = take(ctx->ozws_bytes);
   }
   return RCWA_OK;

@@ -27,6 +27,7 @@ struct rcwa_context {
   unsigned tc = 0;
   unsigned mixed_stages = RCWA_MIXED_ALL;
   int ir_sweeps = 1;
+  int oz_digits = 5;   // 7-bit digits per operand of the int8-slice GEMM
   // refinement workspace of the current sweep chunk (inside ws), see zgesv_ir
   void* irws = nullptr;
   size_t irws_bytes = 0;

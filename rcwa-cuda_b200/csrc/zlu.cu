@@ -671,18 +671,19 @@ int zgesv(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride,
   return lu_solve<double2>(s, n, nrhs, M, ld, stride, batch, piv);
 }
 
-size_t zgesv_ir_ws_bytes(int n, int nrhs, int batch, int sweeps) {
+size_t zgesv_ir_ws_bytes(int n, int nrhs, int batch, int sweeps, int resid_int8) {
   if (n <= 0 || batch <= 0) return 0;
   const size_t sys = (size_t)batch * n;
   size_t b = al256(sys * (size_t)(n + nrhs) * sizeof(float2));    // complex64 [A | B]
   b += al256(sys * (size_t)nrhs * sizeof(double2));                // FP64 residual
   if (sweeps > 1) b += al256(sys * (size_t)nrhs * sizeof(double2));  // FP64 correction
   b += al256((size_t)batch * 2 * sizeof(unsigned));
+  if (resid_int8) b += al256(zgemm_oz_ws_bytes(n, nrhs, n, batch, 6));
   return b + 256;
 }
 
 int zgesv_ir(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stride, int batch, int* piv,
-             uint32_t* status, void* ws, int sweeps) {
+             uint32_t* status, void* ws, int sweeps, int resid_int8) {
   if (n <= 0 || batch <= 0) return RCWA_OK;
   if (sweeps < 1) sweeps = 1;
   const long long sf = (long long)n * (n + nrhs);
@@ -698,6 +699,14 @@ int zgesv_ir(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stri
     w += al256((size_t)batch * sr * sizeof(double2));
   }
   unsigned* nrm = (unsigned*)w;
+  w += al256((size_t)batch * 2 * sizeof(unsigned));
+  void* ozws = resid_int8 ? (void*)w : nullptr;
+  const size_t ozb = resid_int8 ? zgemm_oz_ws_bytes(n, nrhs, n, batch, 6) : 0;
+  int* oz_err = nullptr;
+  if (resid_int8 && !(oz_err = tc_error_flag())) {
+    set_last_error("zgesv_ir: tensor-core error flag unavailable");
+    return RCWA_ERR_CUDA;
+  }
   int rc;
   // FP32 factorisation and first solve on the complex64 copy
   {
@@ -733,6 +742,13 @@ int zgesv_ir(cudaStream_t s, int n, int nrhs, double2* M, int ld, long long stri
     gm.ldc = n;
     gm.sC = sr;
     gm.batch = batch;
+    if (resid_int8) {   // residuals on the int8-slice GEMM with six digits (~43 bits)
+      gm.tc = TC_INT8;
+      gm.digits = 6;
+      gm.ws = ozws;
+      gm.ws_bytes = ozb;
+      return zgemm_oz(s, gm, oz_err);
+    }
     return zgemm(s, gm);
   };
   if ((rc = residual(M + (long long)n * ld, ld, stride))) return rc;

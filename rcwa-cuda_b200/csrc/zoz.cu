@@ -265,8 +265,10 @@ struct OzCfg {
   static constexpr int A_STAGE = 3 * S * OZ_APL;
   static constexpr int B_STAGE = 2 * S * BPL;
   static constexpr int STAGE = A_STAGE + B_STAGE;
-  static constexpr int ST = (3 * STAGE <= 200 * 1024) ? 3 : 2;
-  static constexpr int SMEM = ST * STAGE + 1024;        // + 1 KB alignment slack
+  // three stages when they fit in the 227 KB of dynamic shared memory a CTA
+  // may use (the no-swizzle layout and the bulk copies need 16-byte alignment)
+  static constexpr int ST = (3 * STAGE + 256 <= 227 * 1024 - 512) ? 3 : 2;
+  static constexpr int SMEM = ST * STAGE + 128;         // + alignment slack
   static constexpr uint32_t TMEM_COLS = 512;            // 2 S TN <= 512
   static_assert(2 * S * TN <= 512, "accumulators exceed tensor memory");
 };
@@ -283,7 +285,7 @@ oz_gemm_kernel(int m, int n, int k, int MB, int NB, int KB, double2 alpha, const
   __shared__ __align__(8) uint64_t full[ST], empty[ST], done;
   __shared__ uint32_t tmem_slot;
   __shared__ int s_ok;
-  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
   const int bz = blockIdx.z, mb = blockIdx.y, nb = blockIdx.x;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint8_t* Ab = Aq + ((long long)bz * MB + mb) * KB * (long long)Cfg::A_STAGE;
@@ -427,8 +429,16 @@ oz_gemm_kernel(int m, int n, int k, int MB, int NB, int KB, double2 alpha, const
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS));
 }
 
-constexpr int OZ_S = 4, OZ_TN = 64;
-using OzDefault = OzCfg<OZ_S, OZ_TN>;
+// Digit counts and their tiles: 2 S TN accumulator columns fit in the 512
+// columns of tensor memory.
+template <int S>
+struct OzTile;
+template <>
+struct OzTile<4> { static constexpr int TN = 64; };
+template <>
+struct OzTile<5> { static constexpr int TN = 48; };
+template <>
+struct OzTile<6> { static constexpr int TN = 32; };
 
 size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -436,41 +446,36 @@ struct OzDims {
   int MB, NB, KB;
   size_t a_bytes, b_bytes, sig_bytes, tau_bytes;
 };
+template <int S>
 OzDims oz_dims(int m, int n, int k, int batch) {
+  constexpr int TN = OzTile<S>::TN;
+  using Cfg = OzCfg<S, TN>;
   OzDims d;
   d.MB = (m + OZ_TM - 1) / OZ_TM;
-  d.NB = (n + OZ_TN - 1) / OZ_TN;
+  d.NB = (n + TN - 1) / TN;
   d.KB = (k + OZ_TK - 1) / OZ_TK;
-  d.a_bytes = al256((size_t)batch * d.MB * d.KB * OzDefault::A_STAGE);
-  d.b_bytes = al256((size_t)batch * d.NB * d.KB * OzDefault::B_STAGE);
+  d.a_bytes = al256((size_t)batch * d.MB * d.KB * Cfg::A_STAGE);
+  d.b_bytes = al256((size_t)batch * d.NB * d.KB * Cfg::B_STAGE);
   d.sig_bytes = al256((size_t)batch * d.MB * OZ_TM * sizeof(double));
-  d.tau_bytes = al256((size_t)batch * d.NB * OZ_TN * sizeof(double));
+  d.tau_bytes = al256((size_t)batch * d.NB * TN * sizeof(double));
   return d;
 }
 
-}  // namespace
-
-size_t zgemm_oz_ws_bytes(int m, int n, int k, int batch) {
-  if (m <= 0 || n <= 0 || batch <= 0) return 0;
-  const OzDims d = oz_dims(m, n, k < 1 ? 1 : k, batch);
+template <int S>
+size_t oz_ws_bytes(int m, int n, int k, int batch) {
+  const OzDims d = oz_dims<S>(m, n, k < 1 ? 1 : k, batch);
   return d.a_bytes + d.b_bytes + d.sig_bytes + d.tau_bytes + 256;
 }
 
-int zgemm_oz(cudaStream_t s, const ZGemm& g, int* err) {
-  if (g.m <= 0 || g.n <= 0 || g.batch <= 0) return RCWA_OK;
-  if (g.opA || g.opB) {
-    set_last_error("zgemm_oz: transposed operands are not supported");
-    return RCWA_ERR_INVALID;
-  }
+template <int S>
+int oz_run(cudaStream_t s, const ZGemm& g, int* err) {
+  constexpr int TN = OzTile<S>::TN;
+  using Cfg = OzCfg<S, TN>;
   const int k = g.k < 1 ? 1 : g.k;   // k <= 0: one zero k-step gives C = beta C
-  const OzDims d = oz_dims(g.m, g.n, k, g.batch);
-  const size_t need = zgemm_oz_ws_bytes(g.m, g.n, k, g.batch);
+  const OzDims d = oz_dims<S>(g.m, g.n, k, g.batch);
+  const size_t need = oz_ws_bytes<S>(g.m, g.n, k, g.batch);
   if (!g.ws || g.ws_bytes < need) {
     set_last_error("zgemm_oz: workspace of %zu bytes, %zu needed", g.ws_bytes, need);
-    return RCWA_ERR_INVALID;
-  }
-  if (g.batch > 65535) {
-    set_last_error("zgemm_oz: batch %d exceeds the grid limit", g.batch);
     return RCWA_ERR_INVALID;
   }
   uint8_t* w = (uint8_t*)(((uintptr_t)g.ws + 255) & ~(uintptr_t)255);
@@ -482,22 +487,22 @@ int zgemm_oz(cudaStream_t s, const ZGemm& g, int* err) {
   int dev = 0;
   RCWA_CUDA_TRY(cudaGetDevice(&dev));
   if (dev >= 64 || !attr[dev]) {
-    RCWA_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<OZ_S, OZ_TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       OzDefault::SMEM));
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<S, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       Cfg::SMEM));
     if (dev < 64) attr[dev] = true;
   }
   const int kk = g.k < 0 ? 0 : g.k;
   void* tok = prof_begin(s);
-  oz_split_a<OZ_S><<<dim3(d.MB, g.batch), OZ_TM, 0, s>>>(g.A, g.lda, g.sA, g.m, kk, d.MB, d.KB, Aq, sig);
+  oz_split_a<S><<<dim3(d.MB, g.batch), OZ_TM, 0, s>>>(g.A, g.lda, g.sA, g.m, kk, d.MB, d.KB, Aq, sig);
   count_launch();
   RCWA_LAUNCH_CHECK();
-  oz_split_b<OZ_S, OZ_TN><<<dim3(cdiv_up((long long)d.NB * OZ_TN, 8), g.batch), 256, 0, s>>>(
-      g.B, g.ldb, g.sB, kk, g.n, d.NB, d.KB, Bq, tau);
+  oz_split_b<S, TN><<<dim3(cdiv_up((long long)d.NB * TN, 8), g.batch), 256, 0, s>>>(g.B, g.ldb, g.sB, kk, g.n,
+                                                                                     d.NB, d.KB, Bq, tau);
   count_launch();
   RCWA_LAUNCH_CHECK();
   prof_end(s, tok, "zgemm_oz_split");
   tok = prof_begin(s);
-  oz_gemm_kernel<OZ_S, OZ_TN><<<dim3(d.NB, d.MB, g.batch), OZ_NT, OzDefault::SMEM, s>>>(
+  oz_gemm_kernel<S, TN><<<dim3(d.NB, d.MB, g.batch), OZ_NT, Cfg::SMEM, s>>>(
       g.m, g.n, kk, d.MB, d.NB, d.KB, g.alpha, Aq, sig, Bq, tau, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, g.dr,
       g.sdr, err);
   prof_end(s, tok, "zgemm_oz");
@@ -505,6 +510,37 @@ int zgemm_oz(cudaStream_t s, const ZGemm& g, int* err) {
   count_launch();
   RCWA_LAUNCH_CHECK();
   return RCWA_OK;
+}
+
+}  // namespace
+
+size_t zgemm_oz_ws_bytes(int m, int n, int k, int batch, int digits) {
+  if (m <= 0 || n <= 0 || batch <= 0) return 0;
+  switch (digits) {
+    case 4: return oz_ws_bytes<4>(m, n, k, batch);
+    case 5: return oz_ws_bytes<5>(m, n, k, batch);
+    default: return oz_ws_bytes<6>(m, n, k, batch);
+  }
+}
+
+int zgemm_oz(cudaStream_t s, const ZGemm& g, int* err) {
+  if (g.m <= 0 || g.n <= 0 || g.batch <= 0) return RCWA_OK;
+  if (g.opA || g.opB) {
+    set_last_error("zgemm_oz: transposed operands are not supported");
+    return RCWA_ERR_INVALID;
+  }
+  if (g.batch > 65535) {
+    set_last_error("zgemm_oz: batch %d exceeds the grid limit", g.batch);
+    return RCWA_ERR_INVALID;
+  }
+  switch (g.digits) {
+    case 4: return oz_run<4>(s, g, err);
+    case 5: return oz_run<5>(s, g, err);
+    case 6: return oz_run<6>(s, g, err);
+    default:
+      set_last_error("zgemm_oz: %d digits (4, 5 or 6 supported)", g.digits);
+      return RCWA_ERR_INVALID;
+  }
 }
 
 }  // namespace rcwa

@@ -40,6 +40,7 @@ MIXED_LAYER_LU = 4
 MIXED_STAR_LU = 8
 MIXED_ALL = 15
 MIXED_GEMM_TF32 = 16   # GEMM stages on split-TF32 instead of int8 slices
+MIXED_REFINE_INT8 = 32  # LU refinement residuals on the int8-slice GEMM
 GEOM_LI_RULE = 1   # rcwa_geometry_create_ex: Li's factorization rule
 
 
@@ -97,7 +98,7 @@ _SIGS = {
     "rcwa_context_set_stream": ([_VP, _VP], C.c_int),
     "rcwa_context_synchronize": ([_VP], C.c_int),
     "rcwa_context_kernel_launches": ([_VP, C.POINTER(C.c_uint64)], C.c_int),
-    "rcwa_context_set_mixed": ([_VP, C.c_uint, C.c_int], C.c_int),
+    "rcwa_context_set_mixed": ([_VP, C.c_uint, C.c_int, C.c_int], C.c_int),
     "rcwa_profile_enable": ([C.c_int], C.c_int),
     "rcwa_profile_reset": ([], C.c_int),
     "rcwa_profile_query": ([C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64),
@@ -424,10 +425,11 @@ class Context:
             return lam[0], W[0], int(st[0])
         return lam, W, st
 
-    def set_mixed(self, stages: int = MIXED_ALL, refine_sweeps: int = 1):
-        """Stages run in reduced precision by PREC_MIXED solves on this context
-        and the FP64 refinement sweeps of their LU solves."""
-        _check(self.lib.rcwa_context_set_mixed(self.h, stages, refine_sweeps))
+    def set_mixed(self, stages: int = MIXED_ALL, refine_sweeps: int = 1, gemm_digits: int = 5):
+        """Stages run in reduced precision by PREC_MIXED solves on this context,
+        the FP64 refinement sweeps of their LU solves and the digits per
+        operand of the int8-slice GEMM."""
+        _check(self.lib.rcwa_context_set_mixed(self.h, stages, refine_sweeps, gemm_digits))
 
     def lu_solve(self, A, B, precision: int = PREC_FP64, refine_sweeps: int = 1):
         A = np.asarray(A, dtype=np.complex128)
