@@ -37,7 +37,8 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-METRIC = "solves/s at |dR|,|dT|<=1e-6 (plain FP64 batched sweep; served mixed-prec vs FP64 reported alongside)"
+METRIC = ("solves/s at |dR|,|dT|<=1e-6: plain FP64 batched sweep (value); mixed precision on the same sweep "
+          "(mixed) and served mixed vs FP64 on a Poisson request mix with p50/p99 ms (served)")
 UNIT = "solves/s"
 
 
@@ -56,6 +57,9 @@ def parse():
     ap.add_argument("--m", type=int, default=31, help="c4: harmonic order M (n = 2 M^2)")
     ap.add_argument("--rates", default="100,200,500,1000,2000,5000", help="c5: arrival rates (1/s)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-served", action="store_true", help="skip the served mixed-vs-FP64 block")
+    ap.add_argument("--served-count", type=int, default=160, help="requests per offered rate and precision")
+    ap.add_argument("--served-rates", default="100,1000", help="offered rates (1/s) of the served block")
     return ap.parse_args()
 
 
@@ -264,6 +268,65 @@ def run_batch_workloads(args):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------- served
+def served_block(count, rates, seed=5):
+    """The serving loop under Poisson arrivals: requests drawn from the C3
+    distribution with harmonic orders up to 25 x 25 (n <= 1250), 128^2 grids,
+    the same request list and arrival times for FP64 and mixed precision.
+    Per precision and offered rate: served requests/s (completed / span from
+    the first submit to the last completion), p50 / p99 submit-to-completion
+    latency, requests refused by back-pressure (queue limit 64); for mixed,
+    max |dR|, |dT| against the FP64 result of the same request."""
+    from rcwa_b200 import lib as L, configs as C
+    rng = np.random.default_rng(seed)
+    pbs = [C.c3_request(rng, 128, 25) for _ in range(count)]
+    out = {"workload": f"{count} C3-distributed requests per rate (odd M 5..25, n <= 1250, 1-6 layers, 128^2 "
+                       "grids), Poisson arrivals, 3 lanes, queue limit 64",
+           "rates": []}
+    results = {}
+    for rate in rates:
+        arr = C.poisson_arrivals(rate, count, seed=int(rate))
+        row = {"rate_hz": rate}
+        for prec_name, prec in (("fp64", L.PREC_FP64), ("mixed", L.PREC_MIXED)):
+            srv = L.Server(0, max_batch=64, max_queue=64, precision=prec)
+            try:
+                srv.poll(srv.submit(pbs[0]), pbs[0], wait=True)       # warm-up (plans, pools)
+                t0 = time.perf_counter()
+                tickets = []
+                for pb, ta in zip(pbs, arr):
+                    dt = ta - (time.perf_counter() - t0)
+                    if dt > 0:
+                        time.sleep(dt)
+                    try:
+                        tickets.append(srv.submit(pb))
+                    except L.RcwaError as e:
+                        if e.code != L.RCWA_ERR_BUSY:
+                            raise
+                        tickets.append(None)
+                res = {}
+                for i, (tk, pb) in enumerate(zip(tickets, pbs)):
+                    if tk is not None:
+                        res[i] = srv.poll(tk, pb, wait=True)
+                span = time.perf_counter() - t0
+                info = srv.info()
+            finally:
+                srv.close()
+            done = len(res)
+            results[(rate, prec_name)] = res
+            row[prec_name] = {"served_per_s": done / span, "p50_ms": info["p50_ms"], "p99_ms": info["p99_ms"],
+                              "completed": done, "refused": count - done,
+                              "status_nonzero": int(sum(1 for r in res.values() if r[5] != 0)),
+                              "peak_admitted_gb": info["peak_admitted_bytes"] / 1e9}
+        r64, rmx = results[(rate, "fp64")], results[(rate, "mixed")]
+        common = [i for i in rmx if i in r64 and r64[i][5] == 0 and rmx[i][5] == 0]
+        err = max([max(np.abs(rmx[i][1] - r64[i][1]).max(), np.abs(rmx[i][2] - r64[i][2]).max()) for i in common]
+                  or [None]) if common else None
+        row["mixed"]["max_abs_dR_dT_vs_fp64"] = err
+        row["mixed_over_fp64_served"] = row["mixed"]["served_per_s"] / row["fp64"]["served_per_s"]
+        out["rates"].append(row)
+    return out
+
+
 # --------------------------------------------------------------------------- ours
 def main():
     args = parse()
@@ -362,6 +425,7 @@ def main():
     L.profile_reset()
     stat_h = st_d.cpu().numpy()
     R_h = R_d.cpu().numpy().reshape(B, N)
+    T_h = T_d.cpu().numpy().reshape(B, N)
     tot_h = tot_d.cpu().numpy().reshape(B, 2)
 
     # ---- end to end through the host-buffer ABI (pinned buffers)
@@ -388,6 +452,28 @@ def main():
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     h2d = er_p.numel() * 8 + ur_p.numel() * 8 + t_p.numel() * 8 + B * 40
     d2h = 2 * B * N * 8 + B * 2 * 8 + B * 4
+
+    # ---- the same sweep in mixed precision (library defaults), device-resident
+    def step_mixed():
+        g = ctx.geometry_create(st, par, er_d.data_ptr(), ur_d.data_ptr(), t_d.data_ptr())
+        ctx.solve_sweep_device(g, srcs, L.PREC_MIXED, R_d.data_ptr(), T_d.data_ptr(), tot_d.data_ptr(),
+                               st_d.data_ptr())
+        ctx.geometry_destroy(g)
+
+    mixed_steps = max(1, min(args.steps, 5))
+    step_mixed()
+    barrier()
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0.record(stream)
+    for _ in range(mixed_steps):
+        step_mixed()
+    m1.record(stream)
+    barrier()
+    mixed_ms = max_over_ranks(m0.elapsed_time(m1))
+    stat_m = st_d.cpu().numpy()
+    R_m = R_d.cpu().numpy().reshape(B, N)
+    T_m = T_d.cpu().numpy().reshape(B, N)
+    tot_m = tot_d.cpu().numpy().reshape(B, 2)
 
     if rank != 0:
         if world > 1:
@@ -419,19 +505,13 @@ def main():
                                                     if hess_all[0] else None)
     shares["hess(blocked, incl. its GEMMs)"] = round(hess_all[0] / max(1e-9, prof_step_ms), 4)
 
-    # DRAM traffic per launch of the dominant family, from ncu captures of the
-    # same kernels on this workload (profiles/), scaled by the units per launch
-    traffic, traffic_src = None, None
-    if dom == "schur":
-        per_matrix = (11.669982e9 + 13.266891e9) / 48          # schur24 capture: 48 matrices
-        traffic = per_matrix * 2 * B                             # 2 patterned layers x B sources per launch
-        traffic_src = ("ncu dram__bytes_read+write of schur_kernel on 48 n=450 matrices of this workload "
-                       "(profiles/schur_kernel_c2_n450_batch48.md), scaled to the 2 x %d matrices of one launch" % B)
-    elif dom == "zgemm":
-        per_flop = (155.732992e6 + 52.608e6) / (24 * 8 * 450.0 ** 3)   # dmma24 capture
-        traffic = per_flop * (dfl / dn) if dn else None
-        traffic_src = ("ncu dram bytes of zgemm_dmma_kernel on the 24 x 450^3 Omega^2 GEMM "
-                       "(profiles/zgemm_dmma_c2_omega2_n450_batch24.md), scaled by flops per launch")
+    # DRAM bytes per launch come from ncu captures, which this run does not
+    # take (a capture serialises and replays the kernel): left null here
+    traffic = None
+    # the pipe the dominant family runs on
+    pipe = {"schur": "fp64 (CUDA-core rotations)", "zgemm": "fp64 tensor (DMMA)",
+            "zgemm_rank": "fp64 (CUDA cores)", "hess_panel": "hbm", "trevc": "fp64 (CUDA cores)",
+            "lu_panel": "fp64 (CUDA cores, latency)"}.get(dom, "fp64")
 
     solves = B * args.steps * world
     value = solves / (dev_ms / 1e3)
@@ -474,15 +554,30 @@ def main():
                    "max_abs_dR_dT_vs_oracle": err},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
-        "roofline": {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": zgemm_peak,
+        "roofline": {"kernel": dom, "bound": "fp64", "pipe": pipe, "achieved": achieved, "peak": zgemm_peak,
                      "unit": "TFLOP/s", "frac": (achieved / zgemm_peak) if achieved else None,
-                     "traffic": traffic, "traffic_source": traffic_src,
-                     "peak_source": "cuBLAS ZGEMM 4096^3 (complex128) measured in this run",
+                     "traffic": traffic,
+                     "traffic_note": "null: DRAM bytes per launch need an ncu capture, not taken in this run",
+                     "peak_source": "FP64 ceiling: cuBLAS ZGEMM 4096^3 (complex128) measured in this run "
+                                    "(MEASURED_PEAKS.json holds no FP64 figure)",
                      "launches": dn, "avg_launch_ms": dms / dn if dn else None,
                      "family_time_share": shares, "family_tflops": fam_tflops},
         "cpu_baseline": cpu,
         "clocks": clocks,
     }
+    okm = (stat_h == 0) & (stat_m == 0)
+    line["mixed"] = {
+        "value": B * mixed_steps * world / (mixed_ms / 1e3), "unit": UNIT, "steps": mixed_steps,
+        "ms_per_step": mixed_ms / mixed_steps,
+        "speedup_vs_fp64": (B * mixed_steps / mixed_ms) / (B * args.steps / dev_ms),
+        "max_abs_dR_dT_vs_fp64": float(max(np.abs(R_m[okm] - R_h[okm]).max(), np.abs(T_m[okm] - T_h[okm]).max(),
+                                           np.abs(tot_m[okm] - tot_h[okm]).max())) if okm.any() else None,
+        "stages": "int8-slice tcgen05 GEMMs (5 digits) for the layer-assembly and star-product products; "
+                  "FP64 LU, Omega^2, eigensolver, sqrt, exp and sums",
+    }
+    if not args.no_served:
+        rates = [float(r) for r in args.served_rates.split(",") if r]
+        line["served"] = served_block(args.served_count, rates)
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -50,8 +50,8 @@ extern "C" {
 
 /* ---- precision modes ---------------------------------------------------- */
 #define RCWA_PREC_FP64 0   /* all-FP64 (parity form, reproduces the reference) */
-#define RCWA_PREC_MIXED 1  /* the stages of rcwa_context_set_mixed (default: all) in reduced
-                              precision; FP64 Omega^2, eig, sqrt, exp and efficiency sums */
+#define RCWA_PREC_MIXED 1  /* the stages of rcwa_context_set_mixed (default: the two GEMM stages)
+                              in reduced precision; FP64 Omega^2, eig, sqrt, exp and sums */
 
 /* Stages that RCWA_PREC_MIXED runs in reduced precision.  GEMM stages use the
  * int8-sliced tensor-core GEMM (each row of A and column of B scaled by a
@@ -141,8 +141,10 @@ int rcwa_context_synchronize(rcwa_context* ctx);
 int rcwa_context_kernel_launches(rcwa_context* ctx, uint64_t* count);
 /* Mixed-precision set-up of this context (no reference counterpart: the
  * reference is FP64 only): the RCWA_MIXED_* stages that RCWA_PREC_MIXED runs
- * in reduced precision (default RCWA_MIXED_ALL; 0 makes RCWA_PREC_MIXED an
- * FP64 solve), the FP64 refinement sweeps of its LU solves (1..4, default 1)
+ * in reduced precision (default RCWA_MIXED_LAYER_GEMM | RCWA_MIXED_STAR_GEMM:
+ * on B200 the FP32 LU with an FP64 residual per sweep costs more than the FP64
+ * LU it replaces; 0 makes RCWA_PREC_MIXED an FP64 solve), the FP64
+ * refinement sweeps of its LU solves (1..4, default 1)
  * and the 7-bit digits per operand of the int8-slice GEMM (4, 5 or 6,
  * default 5: about 29, 36 or 43 bits of each product).  Sweeps and batches
  * run through the context use it. */
@@ -222,10 +224,28 @@ int rcwa_geometry_create_shapes(rcwa_context* ctx, int nx, int ny, double lx, do
 int rcwa_solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks,
                      const rcwa_source* sources, const rcwa_params* params, int precision,
                      rcwa_result* out);
-/* Serving loop: a worker thread with its own context on `device` takes all
- * queued requests (up to max_batch) at the start of each batch and solves
- * them with rcwa_solve_batch (continuous batching).  At most max_queue
- * requests wait at a time. */
+/* Serving loop (continuous batching): `lanes` worker threads on `device`,
+ * each with its own context (stream and workspace).  A free lane admits
+ * queued requests in arrival order -- up to max_batch, up to its share of the
+ * device-memory budget (hbm_budget_bytes / lanes), and only while all
+ * requests in flight stay within the budget -- and solves them as one
+ * batched solve (rcwa_solve_batch) on its stream, so batches of different
+ * lanes overlap on the GPU and a request arriving during a long batch starts
+ * on the next free lane.  A request that does not fit waits (later, smaller
+ * ones may pass it during up to 8 admission rounds); one larger than the
+ * whole budget runs alone.  At most max_queue requests wait at a time (RCWA_ERR_BUSY beyond). */
+typedef struct rcwa_server_config {
+  int max_batch;              /* requests per batched solve of a lane (> 0) */
+  int max_queue;              /* waiting requests before RCWA_ERR_BUSY (> 0) */
+  int precision;              /* RCWA_PREC_FP64 or RCWA_PREC_MIXED */
+  int lanes;                  /* concurrent batches, 1..16 (0: 3) */
+  uint64_t hbm_budget_bytes;  /* in-flight footprint limit (0: min(180 GB, 85 % of free memory)) */
+  unsigned mixed_stages;      /* as rcwa_context_set_mixed (0: its defaults) */
+  int refine_sweeps;
+  int gemm_digits;
+} rcwa_server_config;
+int rcwa_server_create_ex(int device, const rcwa_server_config* cfg, rcwa_server** out);
+/* rcwa_server_create_ex with lanes, budget and mixed settings at their defaults. */
 int rcwa_server_create(int device, int max_batch, int max_queue, int precision,
                        rcwa_server** out);
 /* Queues one request; the stack's arrays are copied (the caller may free them
@@ -237,8 +257,16 @@ int rcwa_server_submit(rcwa_server* srv, const rcwa_stack* stack, const rcwa_sou
  * result and the ticket is released.  Returns the request's own code once
  * done; RCWA_ERR_NOTFOUND for an unknown or already collected ticket. */
 int rcwa_server_poll(rcwa_server* srv, uint64_t ticket, int wait, rcwa_result* out, int* done);
-/* Completed requests and their submit-to-completion latency p50 / p99 (ms). */
+/* Completed requests and their submit-to-completion latency p50 / p99 (ms,
+ * over the last 65536 completions). */
 int rcwa_server_stats(rcwa_server* srv, uint64_t* completed, double* p50_ms, double* p99_ms);
+typedef struct rcwa_server_info {
+  uint64_t completed, queued, in_flight, rejected;  /* rejected: RCWA_ERR_BUSY submissions */
+  double p50_ms, p99_ms;
+  uint64_t admitted_bytes, peak_admitted_bytes, budget_bytes;
+  int lanes;
+} rcwa_server_info;
+int rcwa_server_info_get(rcwa_server* srv, rcwa_server_info* out);
 /* Finishes the queued requests, stops the worker, releases the context. */
 int rcwa_server_destroy(rcwa_server* srv);
 
@@ -313,6 +341,19 @@ int rcwa_eig(rcwa_context* ctx, int n, int batch, const rcwa_complex* A, rcwa_co
 #define RCWA_EIG_NOALLOC_MAX_N 128
 int rcwa_eig_noalloc(int n, int batch, const rcwa_complex* A_dev, rcwa_complex* lam_dev,
                      rcwa_complex* W_dev, uint32_t* status_dev, void* cuda_stream);
+/* Host-side fault injection for the eigensolver's bounded QR iteration (the
+ * reference abort()s when ComplexEigenSolver fails, rcwa.cpp:300): the QR
+ * sweeps allowed per eigensolve, in units of max(n, 10), for every later
+ * solve in the process (-1 restores the default 100; 0 makes every matrix
+ * with an undeflated block stop at once with RCWA_STATUS_EIG_NOCONV and NaN
+ * eigenvalues).  Process-wide: not for use while other threads solve. */
+int rcwa_eig_set_sweep_cap(int sweeps_per_n);
+/* Test hook for the int8-slice GEMM's bounded waits (no reference
+ * counterpart): while on (1), its launches leave out their first operand
+ * copy, so the wait for it gives up after about a second, the CTA records the
+ * failure, frees its tensor memory and returns, and the calling entry point
+ * reports RCWA_ERR_CUDA; 0 turns it off.  Process-wide. */
+int rcwa_debug_gemm_inject_timeout(int on);
 /* PartialPivLU solve (the .lu().solve calls of rcwa.cpp): X = A^-1 B, batched. */
 int rcwa_lu_solve(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_complex* A,
                   const rcwa_complex* B, rcwa_complex* X, uint32_t* status);

@@ -83,6 +83,30 @@ size_t geometry_bytes_per_item(const ModeDims& d, int nl, int nx, int ny) {
   return b + 1024;
 }
 
+}  // namespace
+
+size_t problem_bytes(const rcwa_stack& st, const rcwa_params& p, int precision, unsigned mixed_stages,
+                     int ir_sweeps, int gemm_digits) {
+  ModeDims d;
+  d.nxh = p.nx_harmonics;
+  d.nyh = p.ny_harmonics;
+  d.P = 2 * d.nxh + 1;
+  d.Q = 2 * d.nyh + 1;
+  d.N = d.P * d.Q;
+  d.n = 2 * d.N;
+  const size_t G = (size_t)st.nx * st.ny;
+  int np = 0;
+  for (int l = 0; l < st.num_layers; ++l)
+    np += (grid_uniform(st.er + l * G, G) && grid_uniform(st.ur + l * G, G)) ? 0 : 1;
+  rcwa_context probe;   // only the mixed-precision settings are read
+  probe.tc = precision == RCWA_PREC_MIXED ? mixed_stages : 0u;
+  probe.ir_sweeps = ir_sweeps;
+  probe.oz_digits = gemm_digits;
+  return sweep_bytes_per_source(&probe, d, np) + geometry_bytes_per_item(d, st.num_layers, st.nx, st.ny);
+}
+
+namespace {
+
 // One group chunk: items idx0[0..B) share key k0.
 int run_chunk(rcwa_context* ctx, const GroupKey& k0, const std::vector<int>& idx0,
               const rcwa_stack* stacks, const rcwa_source* sources, const rcwa_params* params,

@@ -25,7 +25,7 @@ struct rcwa_context {
   // tensor-core GEMMs, LU stages an FP32 LU with ir_sweeps FP64 refinement
   // sweeps; Omega^2 and the eigensolver stay FP64
   unsigned tc = 0;
-  unsigned mixed_stages = RCWA_MIXED_ALL;
+  unsigned mixed_stages = RCWA_MIXED_LAYER_GEMM | RCWA_MIXED_STAR_GEMM;
   int ir_sweeps = 1;
   int oz_digits = 5;   // 7-bit digits per operand of the int8-slice GEMM
   // refinement workspace of the current sweep chunk (inside ws), see zgesv_ir
@@ -109,6 +109,11 @@ int sweep_chunk_layers(rcwa_context* ctx, const Layers& g, const SourceDev* hsrc
 // Device-side rasterisers (raster.cu).
 int rasterize(rcwa_context* ctx, int nx, int ny, double lx, double ly, int nl,
               const rcwa_layer_shapes* layers, double2* er, double2* ur, double* t_dev);
+// Device bytes one problem occupies while it is solved in a batch (its share
+// of the sweep plan and of the group's geometry), under the given precision
+// settings (batch.cu).
+size_t problem_bytes(const rcwa_stack& st, const rcwa_params& p, int precision, unsigned mixed_stages,
+                     int ir_sweeps, int gemm_digits);
 // n unrelated problems, grouped by shape into batched solves (batch.cu);
 // max_group > 0 caps the solves per batched launch sequence.
 int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_source* sources,

@@ -39,6 +39,7 @@
 // for the epilogue.  Every mbarrier wait is bounded; on time-out the CTA
 // sets the error flag, waits (bounded) for its own copies and MMAs, frees its
 // tensor memory and returns without writing C.
+#include <atomic>
 #include <cstdint>
 
 #include "common.cuh"
@@ -52,7 +53,9 @@ constexpr int OZ_NT = 128;              // threads per CTA
 constexpr int OZ_TM = 128;              // complex rows per CTA tile (= MMA M)
 constexpr int OZ_TK = 32;               // k per step (= int8 MMA K)
 constexpr int OZ_APL = OZ_TM * OZ_TK;   // bytes of one A digit plane block
-constexpr long long OZ_WAIT_CAP = 1LL << 26;
+// every mbarrier wait gives up after this many SM clock cycles (about one
+// second at 1.9 GHz)
+constexpr long long OZ_WAIT_CYCLES = 2000000000LL;
 
 template <int TN>
 constexpr int oz_bpl() { return TN * OZ_TK; }   // bytes of one B digit plane block
@@ -93,7 +96,8 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(bar)));
 }
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
-  for (long long it = 0; it < OZ_WAIT_CAP; ++it) {
+  const long long t0 = clock64();
+  for (;;) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -103,8 +107,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
         : "r"(su32(bar)), "r"(phase)
         : "memory");
     if (ok) return true;
+    if (clock64() - t0 > OZ_WAIT_CYCLES) return false;
   }
-  return false;
 }
 __device__ __forceinline__ void bulk_load(void* sdst, const void* gsrc, uint32_t bytes, uint64_t* bar) {
   asm volatile(
@@ -278,7 +282,8 @@ __global__ void __launch_bounds__(OZ_NT, 1)
 oz_gemm_kernel(int m, int n, int k, int MB, int NB, int KB, double2 alpha, const uint8_t* __restrict__ Aq,
                const double* __restrict__ sig, const uint8_t* __restrict__ Bq, const double* __restrict__ tau,
                double2 beta, double2* __restrict__ C, int ldc, long long sC, const double2* __restrict__ dl,
-               long long sdl, const double2* __restrict__ dr, long long sdr, int* __restrict__ err) {
+               long long sdl, const double2* __restrict__ dr, long long sdr, int* __restrict__ err,
+               int skip_first_copy) {
   using Cfg = OzCfg<S, TN>;
   constexpr int ST = Cfg::ST;
   extern __shared__ uint8_t smem_raw[];
@@ -312,15 +317,16 @@ oz_gemm_kernel(int m, int n, int k, int MB, int NB, int KB, double2 alpha, const
 
   if (tid == 0) {
     bool ok = true;
-    int issued = 0;      // k-steps whose operands were requested
-    int committed = 0;   // k-steps whose MMAs were committed
+    int pending[ST];     // per stage: the k-step whose copy is in flight and not yet waited for, or -1
+    for (int st = 0; st < ST; ++st) pending[st] = -1;
     auto load = [&](int kt) {
       const int st = kt % ST;
+      if (kt == 0 && skip_first_copy) return;   // test hook: k-step 0 never arrives
       uint8_t* sa = smem + st * Cfg::STAGE;
       expect_tx(&full[st], (uint32_t)Cfg::STAGE);
       bulk_load(sa, Ab + (long long)kt * Cfg::A_STAGE, (uint32_t)Cfg::A_STAGE, &full[st]);
       bulk_load(sa + Cfg::A_STAGE, Bb + (long long)kt * Cfg::B_STAGE, (uint32_t)Cfg::B_STAGE, &full[st]);
-      ++issued;
+      pending[st] = kt;
     };
     for (int p = 0; p < ST && p < KB; ++p) load(p);
     constexpr uint32_t IDESC = oz_idesc<TN>();
@@ -333,6 +339,7 @@ oz_gemm_kernel(int m, int n, int k, int MB, int NB, int KB, double2 alpha, const
         load(kt - 1 + ST);
       }
       if (!mbar_wait(&full[st], (uint32_t)((kt / ST) & 1))) { ok = false; break; }
+      pending[st] = -1;
       asm volatile("tcgen05.fence::after_thread_sync;");
       const uint32_t sa = su32(smem + st * Cfg::STAGE), sb = sa + Cfg::A_STAGE;
 #pragma unroll
@@ -355,12 +362,12 @@ oz_gemm_kernel(int m, int n, int k, int MB, int NB, int KB, double2 alpha, const
         }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
           su32(&empty[st])));
-      ++committed;
     }
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(&done)));
     if (!ok) {
       // wait (bounded) for the copies still in flight before the CTA exits
-      for (int kt = committed; kt < issued; ++kt) mbar_wait(&full[kt % ST], (uint32_t)((kt / ST) & 1));
+      for (int st = 0; st < ST; ++st)
+        if (pending[st] >= 0) mbar_wait(&full[st], (uint32_t)((pending[st] / ST) & 1));
       s_ok = 0;
     }
   }
@@ -428,6 +435,10 @@ oz_gemm_kernel(int m, int n, int k, int MB, int NB, int KB, double2 alpha, const
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS));
 }
+
+// Test hook (rcwa_debug_gemm_inject_timeout): launches skip their first
+// operand copy so that the bounded wait for it runs out.
+std::atomic<int> g_inject_timeout{0};
 
 // Digit counts and their tiles: 2 S TN accumulator columns fit in the 512
 // columns of tensor memory.
@@ -504,7 +515,7 @@ int oz_run(cudaStream_t s, const ZGemm& g, int* err) {
   tok = prof_begin(s);
   oz_gemm_kernel<S, TN><<<dim3(d.NB, d.MB, g.batch), OZ_NT, Cfg::SMEM, s>>>(
       g.m, g.n, kk, d.MB, d.NB, d.KB, g.alpha, Aq, sig, Bq, tau, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, g.dr,
-      g.sdr, err);
+      g.sdr, err, g_inject_timeout.load() ? 1 : 0);
   prof_end(s, tok, "zgemm_oz");
   if (tok) prof_add_flops("zgemm_oz", 8.0 * g.m * (double)g.n * (double)kk * g.batch);
   count_launch();
@@ -544,3 +555,8 @@ int zgemm_oz(cudaStream_t s, const ZGemm& g, int* err) {
 }
 
 }  // namespace rcwa
+
+extern "C" int rcwa_debug_gemm_inject_timeout(int on) {
+  rcwa::g_inject_timeout.store(on ? 1 : 0);
+  return RCWA_OK;
+}

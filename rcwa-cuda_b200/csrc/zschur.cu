@@ -27,6 +27,8 @@
 // warps apply the logged reflectors to the columns right of the window, the
 // rows above it and to Z, each thread streaming one row or column through
 // registers.
+#include <atomic>
+
 #include "common.cuh"
 #include "eig_common.cuh"
 #include "kernels.cuh"
@@ -919,6 +921,10 @@ extern "C" int rcwa_debug_schur_stats(unsigned long long* out, int reset) {
 }
 #endif
 
+// QR sweeps allowed per eigensolve, in units of max(n, 10): 100 unless a
+// caller lowers it (rcwa_eig_set_sweep_cap, host-side fault injection)
+static std::atomic<int> g_sweeps_per_n{100};
+
 int schur_launch(cudaStream_t s, double2* H, int ld, long long sH, int n, double2* Z, double2* lam,
                  long long slam, uint32_t* status, int batch) {
   void* tok = prof_begin(s);
@@ -931,7 +937,7 @@ int schur_launch(cudaStream_t s, double2* H, int ld, long long sH, int n, double
                                        (int)stage_bytes));
     if (dev < 64) attr_set[dev] = true;
   }
-  schur_kernel<<<batch, NT, stage_bytes, s>>>(H, ld, sH, n, Z, lam, slam, status, 100);
+  schur_kernel<<<batch, NT, stage_bytes, s>>>(H, ld, sH, n, Z, lam, slam, status, g_sweeps_per_n.load());
   prof_end(s, tok, "schur");
   // work convention: eig with vectors = 100 n^3 real flops per complex matrix,
   // of which Hessenberg (40/3), Q (16/3), triangular vectors (4/3) and the
@@ -944,3 +950,12 @@ int schur_launch(cudaStream_t s, double2* H, int ld, long long sH, int n, double
 }
 
 }  // namespace rcwa
+
+extern "C" int rcwa_eig_set_sweep_cap(int sweeps_per_n) {
+  if (sweeps_per_n < -1) {
+    rcwa::set_last_error("sweeps_per_n must be -1 (default) or >= 0");
+    return RCWA_ERR_INVALID;
+  }
+  rcwa::g_sweeps_per_n.store(sweeps_per_n < 0 ? 100 : sweeps_per_n);
+  return RCWA_OK;
+}

@@ -84,6 +84,19 @@ class CLayerShapes(C.Structure):
 SHAPE_CIRCLE, SHAPE_RECT, SHAPE_LINES, SHAPE_TRIANGLE = 1, 2, 3, 4
 
 
+class CServerConfig(C.Structure):
+    _fields_ = [("max_batch", C.c_int), ("max_queue", C.c_int), ("precision", C.c_int), ("lanes", C.c_int),
+                ("hbm_budget_bytes", C.c_uint64), ("mixed_stages", C.c_uint), ("refine_sweeps", C.c_int),
+                ("gemm_digits", C.c_int)]
+
+
+class CServerInfo(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("queued", C.c_uint64), ("in_flight", C.c_uint64),
+                ("rejected", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("admitted_bytes", C.c_uint64), ("peak_admitted_bytes", C.c_uint64),
+                ("budget_bytes", C.c_uint64), ("lanes", C.c_int)]
+
+
 class CResult(C.Structure):
     _fields_ = [("R", C.c_void_p), ("T", C.c_void_p), ("R_tot", C.c_double),
                 ("T_tot", C.c_double), ("status", C.c_uint32)]
@@ -126,6 +139,8 @@ _SIGS = {
                            C.POINTER(CResult)], C.c_int),
     "rcwa_eig": ([_VP, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_eig_noalloc": ([C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP], C.c_int),
+    "rcwa_eig_set_sweep_cap": ([C.c_int], C.c_int),
+    "rcwa_debug_gemm_inject_timeout": ([C.c_int], C.c_int),
     "rcwa_lu_solve": ([_VP, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_lu_solve_ex": ([_VP, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP, C.c_int, C.c_int], C.c_int),
     "rcwa_gemm_ex": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, CComplex, _VP, _VP,
@@ -138,6 +153,8 @@ _SIGS = {
     "rcwa_solve_batch": ([_VP, C.c_int, C.POINTER(CStack), C.POINTER(CSource), C.POINTER(CParams),
                           C.c_int, C.POINTER(CResult)], C.c_int),
     "rcwa_server_create": ([C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_VP)], C.c_int),
+    "rcwa_server_create_ex": ([C.c_int, C.POINTER(CServerConfig), C.POINTER(_VP)], C.c_int),
+    "rcwa_server_info_get": ([_VP, C.POINTER(CServerInfo)], C.c_int),
     "rcwa_server_submit": ([_VP, C.POINTER(CStack), C.POINTER(CSource), C.POINTER(CParams),
                             C.POINTER(C.c_uint64)], C.c_int),
     "rcwa_server_poll": ([_VP, C.c_uint64, C.c_int, C.POINTER(CResult), C.POINTER(C.c_int)], C.c_int),
@@ -561,10 +578,21 @@ class Server:
     """``rcwa_server_*``: a serving loop with continuous batching on one GPU."""
 
     def __init__(self, device: int = 0, max_batch: int = 256, max_queue: int = 100000,
-                 precision: int = PREC_FP64):
+                 precision: int = PREC_FP64, lanes: int = 0, hbm_budget_bytes: int = 0,
+                 mixed_stages: int = 0, refine_sweeps: int = 0, gemm_digits: int = 0):
         self.lib = load()
         self.h = C.c_void_p()
-        _check(self.lib.rcwa_server_create(device, max_batch, max_queue, precision, C.byref(self.h)))
+        cfg = CServerConfig(max_batch, max_queue, precision, lanes, int(hbm_budget_bytes), mixed_stages,
+                            refine_sweeps, gemm_digits)
+        _check(self.lib.rcwa_server_create_ex(device, C.byref(cfg), C.byref(self.h)))
+
+    def info(self) -> dict:
+        """Counters of the server: completed / queued / in-flight / rejected
+        requests, latency p50 / p99 (ms), admitted and peak admitted device
+        bytes against the budget, lanes."""
+        i = CServerInfo()
+        _check(self.lib.rcwa_server_info_get(self.h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in CServerInfo._fields_}
 
     def submit(self, pb: Problem, source_index: int = 0) -> int:
         st = pb.stack

@@ -22,6 +22,15 @@ Cases:
                       trapezoidal posts on a film over a lossy substrate,
                       rcwa_b200.configs.c4_trapezoid) at M = 23 (n = 1058),
                       512 x 512 grids, one wavelength (600 nm), TM.
+  golden_c4_m23_sweep the same stack at 250, 430 and 800 nm (the ends and the
+                      middle of the C4 band).
+  golden_c4_m31       the same stack at the largest C4 order, M = 31
+                      (n = 1922), at 300 and 700 nm.
+  golden_c3_full_<i>  requests i = 0, 1, 2 of the C3 distribution restricted
+                      to its largest orders (odd M in 15..21, n = 450..882),
+                      256 x 256 grids, drawn with numpy default_rng(2121).
+
+    python tests/golden/make_golden.py golden_c4_m31   (one case)
 """
 from __future__ import annotations
 
@@ -38,7 +47,8 @@ for p in (ROOT, os.path.join(ROOT, "rcwa-cuda_b200"), os.path.dirname(HERE)):
 
 from rcwa_b200 import configs as C  # noqa: E402
 
-CASES = ("golden_small_c1", "golden_small_mixed", "golden_c4_m23")
+CASES = ("golden_small_c1", "golden_small_mixed", "golden_c4_m23", "golden_c4_m23_sweep", "golden_c4_m31",
+         "golden_c3_full_0", "golden_c3_full_1", "golden_c3_full_2")
 
 
 def build_case(name: str) -> C.Problem:
@@ -64,12 +74,21 @@ def build_case(name: str) -> C.Problem:
                          C.ParamSpec(3, 2, 1.0, 1.0, C.ref_eps(complex(2.25, 0.01)), 1.0))
     if name == "golden_c4_m23":
         return C.c4_trapezoid(M=23, lambdas=[600.0])
+    if name == "golden_c4_m23_sweep":
+        return C.c4_trapezoid(M=23, lambdas=[250.0, 430.0, 800.0])
+    if name == "golden_c4_m31":
+        return C.c4_trapezoid(M=31, lambdas=[300.0, 700.0])
+    if name.startswith("golden_c3_full_"):
+        i = int(name.rsplit("_", 1)[1])
+        rng = np.random.default_rng(2121)
+        pbs = [C.c3_request(rng, grid=256, m_max=21, m_min=15) for _ in range(i + 1)]
+        return pbs[i]
     raise KeyError(name)
 
 
 def main() -> None:
     from helpers import oracle_sweep
-    for name in CASES:
+    for name in (sys.argv[1:] or CASES):
         pb = build_case(name)
         res = oracle_sweep(pb)
         np.savez_compressed(os.path.join(HERE, name + ".npz"),

@@ -316,10 +316,13 @@ def test_zero_thickness_and_single_uniform(ctx):
     assert np.abs(a[0] - b[0]).max() < 1e-11 and np.abs(a[1] - b[1]).max() < 1e-11
 
 
-@pytest.mark.parametrize("name", ["golden_small_c1", "golden_small_mixed", "golden_c4_m23"])
+@pytest.mark.parametrize("name", ["golden_small_c1", "golden_small_mixed", "golden_c4_m23", "golden_c4_m23_sweep",
+                                  "golden_c4_m31", "golden_c3_full_0", "golden_c3_full_1", "golden_c3_full_2"])
 def test_golden_fixtures(ctx, name):
     """The CUDA path reproduces the committed fixtures (generated by the
-    oracle, tests/golden/make_golden.py) to 1e-10 per order."""
+    oracle, tests/golden/make_golden.py) to 1e-10 per order: small cases, the
+    C4 stack at M = 23 (n = 1058, four wavelengths) and M = 31 (n = 1922, two
+    wavelengths), and full-size C3 requests (M = 15..21, 256^2 grids)."""
     import os
     from golden.make_golden import build_case
     z = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
