@@ -50,9 +50,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n-lambda", type=int, default=201)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "gemm"],
                     help="c2: the headline sweep (default); c3: batch of uneven requests; "
-                         "c4: large-n precision-stress sweep; c5: Poisson-served requests")
+                         "c4: large-n precision-stress sweep; c5: Poisson-served requests; "
+                         "gemm: the complex GEMM kernels at the sweep's shape")
+    ap.add_argument("--gemm-batch", type=int, default=64, help="gemm: matrices per batched product")
     ap.add_argument("--count", type=int, default=0, help="c3/c5: number of requests (0 = workload default)")
     ap.add_argument("--m", type=int, default=31, help="c4: harmonic order M (n = 2 M^2)")
     ap.add_argument("--rates", default="100,200,500,1000,2000,5000", help="c5: arrival rates (1/s)")
@@ -187,7 +189,43 @@ def run_batch_workloads(args):
     ctx.set_stream(stream.cuda_stream)
     line = {"n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "c128", "data": "synthetic", "precision": args.precision}
-    if args.workload == "c3":
+    if args.workload == "gemm":
+        # C = A B, n = 450 (the C2 layer size), device-resident operands, each
+        # kernel timed with CUDA events over args.steps launches
+        n, b = 450, args.gemm_batch
+        A = torch.randn(b, n, n, dtype=torch.complex128, device="cuda")
+        Bm = torch.randn(b, n, n, dtype=torch.complex128, device="cuda")
+        Cm = torch.empty(b, n, n, dtype=torch.complex128, device="cuda")
+        ref = torch.matmul(A, Bm)
+        # the library is column-major: pass the transposes' storage, C^T = B^T A^T
+        At, Bt = A.transpose(1, 2).contiguous(), Bm.transpose(1, 2).contiguous()
+        rows = []
+        variants = [("fp64 DMMA", L.PREC_FP64, 0, 5), ("int8 slices S=4", L.PREC_MIXED, 3, 4),
+                    ("int8 slices S=5", L.PREC_MIXED, 3, 5), ("int8 slices S=6", L.PREC_MIXED, 3, 6),
+                    ("split-TF32", L.PREC_MIXED, 3 | L.MIXED_GEMM_TF32, 5)]
+        for name, prec, stages, dg in variants:
+            ctx.set_mixed(stages or 3, 1, dg)
+            for _ in range(args.warmup):
+                ctx.gemm_device(At.data_ptr(), Bt.data_ptr(), Cm.data_ptr(), n, n, n, b, prec)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                ctx.gemm_device(At.data_ptr(), Bt.data_ptr(), Cm.data_ptr(), n, n, n, b, prec)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            got = Cm.transpose(1, 2)
+            err = float((got - ref).abs().max() / ref.abs().max())
+            rows.append({"kernel": name, "ms": ms, "tflops": 8.0 * n ** 3 * b / (ms / 1e3) / 1e12,
+                         "rel_err": err})
+        ctx.set_mixed(3, 1, 5)
+        line.update({"metric": "complex GEMM TFLOP/s (8 m n k per product) at n = 450",
+                     "value": max(r["tflops"] for r in rows if r["kernel"] != "fp64 DMMA"),
+                     "unit": "TFLOP/s", "steps": args.steps, "warmup": args.warmup,
+                     "config": {"workload": f"{b} x (450 x 450) x (450 x 450) complex products, device-resident",
+                                "kernels": rows}})
+    elif args.workload == "c3":
         count = args.count or 4096
         pbs = C.c3_batch(count=count)
         ctx.solve_batch(pbs[:32], precision=prec)          # warm-up (plans, pools)

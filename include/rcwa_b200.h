@@ -369,6 +369,11 @@ int rcwa_lu_solve_ex(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_c
  * rcwa.cpp). */
 int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_complex* A,
               const rcwa_complex* B, rcwa_complex* C, int precision);
+/* rcwa_gemm on device arrays (batch-packed, column-major), asynchronous on
+ * the context's stream; the mixed-precision GEMM's workspace comes from the
+ * context's workspace. */
+int rcwa_gemm_device(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_complex* A_dev,
+                     const rcwa_complex* B_dev, rcwa_complex* C_dev, int precision);
 /* C = alpha op(A) op(B) + beta C, batched, column-major host arrays; op = 1
  * takes the conjugate transpose (A stored k x m, B stored n x k), C is read
  * when beta != 0.  FP64 only. */

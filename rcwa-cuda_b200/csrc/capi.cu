@@ -560,6 +560,27 @@ int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_comp
   return RCWA_OK;
 }
 
+int rcwa_gemm_device(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_complex* A,
+                     const rcwa_complex* B, rcwa_complex* C, int precision) {
+  CHECK_ARG(ctx && A && B && C && m > 0 && n > 0 && k > 0 && batch > 0, "bad argument");
+  CHECK_ARG(precision == RCWA_PREC_FP64 || precision == RCWA_PREC_MIXED, "unknown precision mode");
+  RCWA_CUDA_TRY(cudaSetDevice(ctx->device));
+  const int kind = precision != RCWA_PREC_MIXED ? 0 : (ctx->mixed_stages & RCWA_MIXED_GEMM_TF32) ? TC_TF32 : TC_INT8;
+  const size_t wsb = kind == TC_INT8 ? zgemm_oz_ws_bytes(m, n, k, batch, ctx->oz_digits) : 0;
+  int rc = ctx_reserve(ctx, wsb + 1024);
+  if (rc) return rc;
+  ZGemm g;
+  g.m = m; g.n = n; g.k = k; g.batch = batch;
+  g.A = (const double2*)A; g.lda = m; g.sA = (long long)m * k;
+  g.B = (const double2*)B; g.ldb = k; g.sB = (long long)k * n;
+  g.C = (double2*)C; g.ldc = m; g.sC = (long long)m * n;
+  g.tc = kind;
+  g.digits = ctx->oz_digits;
+  g.ws = ctx->ws;
+  g.ws_bytes = wsb;
+  return zgemm(ctx->stream, g);
+}
+
 int rcwa_gemm_ex(rcwa_context* ctx, int opa, int opb, int m, int n, int k, int batch,
                  rcwa_complex alpha, const rcwa_complex* A, const rcwa_complex* B, rcwa_complex beta,
                  rcwa_complex* C) {

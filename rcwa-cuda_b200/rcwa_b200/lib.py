@@ -146,6 +146,7 @@ _SIGS = {
     "rcwa_gemm_ex": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, CComplex, _VP, _VP,
                       CComplex, _VP], C.c_int),
     "rcwa_gemm": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, C.c_int], C.c_int),
+    "rcwa_gemm_device": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, C.c_int], C.c_int),
     "rcwa_rasterize": ([_VP, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.POINTER(CLayerShapes),
                         _VP, _VP, _VP], C.c_int),
     "rcwa_geometry_create_shapes": ([_VP, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
@@ -481,6 +482,11 @@ class Context:
         _check(self.lib.rcwa_gemm(self.h, m, n, k, b, _ptr(Af), _ptr(Bf), _ptr(Cf), precision))
         Cm = Cf.transpose(0, 2, 1)
         return Cm[0] if single else Cm
+
+    def gemm_device(self, A_ptr, B_ptr, C_ptr, m, n, k, batch, precision: int = PREC_FP64):
+        """``rcwa_gemm_device``: C = A B on batch-packed column-major device
+        arrays, asynchronous on the context's stream."""
+        _check(self.lib.rcwa_gemm_device(self.h, m, n, k, batch, A_ptr, B_ptr, C_ptr, precision))
 
     def gemm_ex(self, A, B, C=None, opa=0, opb=0, alpha=1.0, beta=0.0):
         """``rcwa_gemm_ex``: alpha op(A) op(B) + beta C on [b, rows, cols]
