@@ -110,7 +110,7 @@ namespace {
 // One group chunk: items idx0[0..B) share key k0.
 int run_chunk(rcwa_context* ctx, const GroupKey& k0, const std::vector<int>& idx0,
               const rcwa_stack* stacks, const rcwa_source* sources, const rcwa_params* params,
-              rcwa_result* out, bool& any_status) {
+              rcwa_result* out, bool& any_status, const ChunkSink* sink) {
   cudaStream_t s = ctx->stream;
   const int B = (int)idx0.size();
   // the chunk's budget comes from its own context (workers get a share)
@@ -285,13 +285,24 @@ int run_chunk(rcwa_context* ctx, const GroupKey& k0, const std::vector<int>& idx
     o.status = hst[b];
     any_status = any_status || hst[b] != 0;
   }
+  if (ctx->tc) {   // a mixed-precision chunk is only handed out once its tensor-core waits all held
+    int* terr = tc_error_flag();
+    int h = 0;
+    if (terr) RCWA_CUDA_TRY(cudaMemcpy(&h, terr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+      set_last_error("tensor-core GEMM: a bounded mbarrier wait expired");
+      return RCWA_ERR_CUDA;
+    }
+  }
+  if (sink && sink->fn) sink->fn(sink->user, idx.data(), B);
   return RCWA_OK;
 }
 
 }  // namespace
 
 int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_source* sources,
-                const rcwa_params* params, int precision, int max_group, rcwa_result* out) {
+                const rcwa_params* params, int precision, int max_group, rcwa_result* out,
+                const ChunkSink* sink) {
   if (precision != RCWA_PREC_FP64 && precision != RCWA_PREC_MIXED) {
     set_last_error("unknown precision mode %d", precision);
     return RCWA_ERR_INVALID;
@@ -399,7 +410,7 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
   if (K <= 1) {
     for (const Job& j : jobs) {
       bool st = false;
-      int rc = run_chunk(ctx, keys[j.g], j.idx, stacks, sources, params, out, st);
+      int rc = run_chunk(ctx, keys[j.g], j.idx, stacks, sources, params, out, st, sink);
       if (st) any_status = true;
       if (rc) return rc;
     }
@@ -443,7 +454,7 @@ int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_s
         }
         for (int j : bins[w]) {
           bool st = false;
-          int r = run_chunk(wc, keys[jobs[j].g], jobs[j].idx, stacks, sources, params, out, st);
+          int r = run_chunk(wc, keys[jobs[j].g], jobs[j].idx, stacks, sources, params, out, st, sink);
           if (st) any_status = true;
           if (r) {
             rcs[w] = r;

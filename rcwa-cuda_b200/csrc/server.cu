@@ -126,6 +126,47 @@ std::vector<Request*> admit(rcwa_server* S) {
   return batch;
 }
 
+// Marks requests done and records their latency (caller holds the lock).
+void finish(rcwa_server* S, Request* r, const rcwa_result& o, int rc, const std::string& msg,
+            Clock::time_point now) {
+  if (r->done) return;
+  r->R_tot = o.R_tot;
+  r->T_tot = o.T_tot;
+  r->status = o.status;
+  if (rc == RCWA_OK || rc == RCWA_ERR_NUMERIC)
+    r->rc = o.status ? RCWA_ERR_NUMERIC : RCWA_OK;
+  else {
+    r->rc = rc;
+    r->err = msg;
+  }
+  r->done = true;
+  r->t_done = now;
+  S->lat.add(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
+  S->admitted -= r->bytes;
+  S->in_flight -= 1;
+  S->completed += 1;
+}
+
+// A lane's batch while it is solved: the chunk callback of solve_batch
+// completes its requests group by group.
+struct LaneBatch {
+  rcwa_server* S;
+  const std::vector<Request*>* batch;
+  const std::vector<rcwa_result>* out;
+};
+
+void chunk_done(void* user, const int* idx, int count) {
+  LaneBatch* lb = static_cast<LaneBatch*>(user);
+  const auto now = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(lb->S->mu);
+    for (int q = 0; q < count; ++q)
+      finish(lb->S, (*lb->batch)[idx[q]], (*lb->out)[idx[q]], RCWA_OK, std::string(), now);
+  }
+  lb->S->cv_done.notify_all();
+  lb->S->cv_work.notify_all();   // freed memory may admit waiting requests on other lanes
+}
+
 void serve(rcwa_server* S, int lane) {
   cudaSetDevice(S->device);
   rcwa_context* ctx = S->ctx[lane];
@@ -147,7 +188,7 @@ void serve(rcwa_server* S, int lane) {
       }
     }
     const int n = (int)batch.size();
-    size_t bytes = 0;
+    size_t bytes = 0;   // the batch's footprint: sizes its chunks
     st.resize(n);
     src.resize(n);
     par.resize(n);
@@ -165,33 +206,21 @@ void serve(rcwa_server* S, int lane) {
     }
     // the batch's chunks are sized for what was admitted for it
     ctx->mem_budget = std::max<size_t>(bytes + (bytes >> 3), (size_t)1 << 28);
+    LaneBatch lb{S, &batch, &out};
+    rcwa::ChunkSink sink;
+    sink.fn = chunk_done;
+    sink.user = &lb;
     const int rc = rcwa::solve_batch(ctx, n, st.data(), src.data(), par.data(), S->precision, S->max_batch,
-                                     out.data());
+                                     out.data(), &sink);
     const std::string msg = (rc == RCWA_OK || rc == RCWA_ERR_NUMERIC) ? std::string() : rcwa_last_error();
     const auto now = Clock::now();
     {
+      // requests of chunks that did not complete carry the batch's error
       std::lock_guard<std::mutex> lk(S->mu);
-      for (int i = 0; i < n; ++i) {
-        Request* r = batch[i];
-        r->R_tot = out[i].R_tot;
-        r->T_tot = out[i].T_tot;
-        r->status = out[i].status;
-        if (rc == RCWA_OK || rc == RCWA_ERR_NUMERIC)
-          r->rc = out[i].status ? RCWA_ERR_NUMERIC : RCWA_OK;
-        else {
-          r->rc = rc;
-          r->err = msg;
-        }
-        r->done = true;
-        r->t_done = now;
-        S->lat.add(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
-      }
-      S->admitted -= bytes;
-      S->in_flight -= n;
-      S->completed += n;
+      for (int i = 0; i < n; ++i) finish(S, batch[i], out[i], rc == RCWA_OK ? RCWA_ERR_CUDA : rc, msg, now);
     }
     S->cv_done.notify_all();
-    S->cv_work.notify_all();   // freed memory may admit waiting requests on other lanes
+    S->cv_work.notify_all();
   }
 }
 

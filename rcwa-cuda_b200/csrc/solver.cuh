@@ -114,10 +114,18 @@ int rasterize(rcwa_context* ctx, int nx, int ny, double lx, double ly, int nl,
 // settings (batch.cu).
 size_t problem_bytes(const rcwa_stack& st, const rcwa_params& p, int precision, unsigned mixed_stages,
                      int ir_sweeps, int gemm_digits);
+// Told about every group chunk of a batch as soon as its results are in
+// out[] (called from the batch's worker threads): idx holds the count
+// problem indices of the chunk.
+struct ChunkSink {
+  void (*fn)(void* user, const int* idx, int count) = nullptr;
+  void* user = nullptr;
+};
 // n unrelated problems, grouped by shape into batched solves (batch.cu);
 // max_group > 0 caps the solves per batched launch sequence.
 int solve_batch(rcwa_context* ctx, int n, const rcwa_stack* stacks, const rcwa_source* sources,
-                const rcwa_params* params, int precision, int max_group, rcwa_result* out);
+                const rcwa_params* params, int precision, int max_group, rcwa_result* out,
+                const ChunkSink* sink = nullptr);
 
 // Build convolution matrices and their inverses.  grids_er/ur are device
 // pointers ([nl][ny][nx]) when on_device, host pointers otherwise.
