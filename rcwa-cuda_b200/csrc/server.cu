@@ -126,10 +126,11 @@ std::vector<Request*> admit(rcwa_server* S) {
   return batch;
 }
 
-// Marks requests done and records their latency (caller holds the lock).
+// Marks a request done and records its latency (caller holds the lock).
+// Once done, a client may collect the request and free it at any time: the
+// lane never touches it again (LaneBatch::fin).
 void finish(rcwa_server* S, Request* r, const rcwa_result& o, int rc, const std::string& msg,
             Clock::time_point now) {
-  if (r->done) return;
   r->R_tot = o.R_tot;
   r->T_tot = o.T_tot;
   r->status = o.status;
@@ -153,6 +154,7 @@ struct LaneBatch {
   rcwa_server* S;
   const std::vector<Request*>* batch;
   const std::vector<rcwa_result>* out;
+  std::vector<char>* fin;   // request i already finished (guarded by S->mu)
 };
 
 void chunk_done(void* user, const int* idx, int count) {
@@ -160,8 +162,12 @@ void chunk_done(void* user, const int* idx, int count) {
   const auto now = Clock::now();
   {
     std::lock_guard<std::mutex> lk(lb->S->mu);
-    for (int q = 0; q < count; ++q)
-      finish(lb->S, (*lb->batch)[idx[q]], (*lb->out)[idx[q]], RCWA_OK, std::string(), now);
+    for (int q = 0; q < count; ++q) {
+      const int i = idx[q];
+      if ((*lb->fin)[i]) continue;
+      (*lb->fin)[i] = 1;
+      finish(lb->S, (*lb->batch)[i], (*lb->out)[i], RCWA_OK, std::string(), now);
+    }
   }
   lb->S->cv_done.notify_all();
   lb->S->cv_work.notify_all();   // freed memory may admit waiting requests on other lanes
@@ -206,7 +212,8 @@ void serve(rcwa_server* S, int lane) {
     }
     // the batch's chunks are sized for what was admitted for it
     ctx->mem_budget = std::max<size_t>(bytes + (bytes >> 3), (size_t)1 << 28);
-    LaneBatch lb{S, &batch, &out};
+    std::vector<char> fin(n, 0);
+    LaneBatch lb{S, &batch, &out, &fin};
     rcwa::ChunkSink sink;
     sink.fn = chunk_done;
     sink.user = &lb;
@@ -217,7 +224,11 @@ void serve(rcwa_server* S, int lane) {
     {
       // requests of chunks that did not complete carry the batch's error
       std::lock_guard<std::mutex> lk(S->mu);
-      for (int i = 0; i < n; ++i) finish(S, batch[i], out[i], rc == RCWA_OK ? RCWA_ERR_CUDA : rc, msg, now);
+      for (int i = 0; i < n; ++i)
+        if (!fin[i]) {
+          fin[i] = 1;
+          finish(S, batch[i], out[i], rc == RCWA_OK ? RCWA_ERR_CUDA : rc, msg, now);
+        }
     }
     S->cv_done.notify_all();
     S->cv_work.notify_all();
