@@ -348,6 +348,12 @@ int rcwa_eig_noalloc(int n, int batch, const rcwa_complex* A_dev, rcwa_complex* 
  * with an undeflated block stop at once with RCWA_STATUS_EIG_NOCONV and NaN
  * eigenvalues).  Process-wide: not for use while other threads solve. */
 int rcwa_eig_set_sweep_cap(int sweeps_per_n);
+/* CTAs that share one matrix in the eigensolver's QR iteration (no
+ * reference counterpart): 0 (default) chooses per launch -- for n >= 400 in
+ * launches of few matrices, a thread-block cluster of up to 8 CTAs whose
+ * helpers share the far updates of each multishift sweep -- while 1, 2, 4 or
+ * 8 forces that many (if the device can hold such clusters).  Process-wide. */
+int rcwa_eig_set_cluster_size(int ctas_per_matrix);
 /* Test hook for the int8-slice GEMM's bounded waits (no reference
  * counterpart): while on (1), its launches leave out their first operand
  * copy, so the wait for it gives up after about a second, the CTA records the

@@ -29,6 +29,8 @@
 // registers.
 #include <atomic>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "eig_common.cuh"
 #include "kernels.cuh"
@@ -80,7 +82,29 @@ struct Smem {
   int l;
   int flag;
   double2 shift;
+  // cluster mode: the command the leader CTA posts to its helpers before a
+  // barrier (1 = multishift sweep over [cmd_l, cmd_i], 0 = done)
+  int cmd, cmd_l, cmd_i;
 };
+
+// Barrier of the CTAs that share one matrix.  One CTA: __syncthreads.  A
+// cluster of CL CTAs: a cluster barrier, with device-scope fences on both
+// sides so that the global-memory updates of H and Z made by one CTA are
+// seen by the others after it.
+template <int CL>
+__device__ __forceinline__ void mat_sync() {
+  if constexpr (CL > 1) {
+    __threadfence();
+    cooperative_groups::this_cluster().sync();
+    __threadfence();
+  } else {
+    __syncthreads();
+  }
+}
+// Update warps of a matrix: the leader's 7 (its warp 0 chases) plus 8 per
+// helper CTA.
+template <int CL>
+constexpr int update_warps() { return NT / 32 - 1 + (NT / 32) * (CL - 1); }
 
 // Shared-memory loads the compiler may not hoist out of the per-row loops of
 // the deferred updates (hoisting all logged reflectors would spill registers).
@@ -427,7 +451,15 @@ __device__ __noinline__ void ms_apply_rows(const Smem& sm, int buf, double2* H, 
 // window c and Z.  Window c+1 never overlaps what warps 1.. touch in that
 // iteration: their columns lie right of window c+1, their rows above
 // window c.
+//
+// With CL > 1 CTAs per matrix (a thread-block cluster) the far updates are
+// shared: the leader CTA (this function) posts the sweep to its helpers
+// (schur_helper) and every chunk ends with a cluster barrier instead of a
+// CTA barrier; update warp g of NG = update_warps<CL>() takes columns and rows
+// g, g + NG, ...
+template <int CL>
 __device__ void multi_sweep(Smem& sm, double2* stage, double2* H, double2* Z, int ld, int n, int l, int i) {
+  constexpr int NG = update_warps<CL>();
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int T = (i - l) + 2 * (NS - 1);
   const int C = (T + MW - 1) / MW;
@@ -445,6 +477,14 @@ __device__ void multi_sweep(Smem& sm, double2* stage, double2* H, double2* Z, in
     __syncthreads();
     store_window(sm, H, ld, j0, j1 - j0 + 1);
     __syncthreads();
+  }
+  if constexpr (CL > 1) {   // post the sweep; chunk 0's log is ready for the helpers
+    if (tid == 0) {
+      sm.cmd = 1;
+      sm.cmd_l = l;
+      sm.cmd_i = i;
+    }
+    mat_sync<CL>();
   }
   for (int c = 0; c < C; ++c) {
     const int buf = c & 1;
@@ -475,15 +515,56 @@ __device__ void multi_sweep(Smem& sm, double2* stage, double2* H, double2* Z, in
       }
       SCHUR_STAT_T(0, 8, clock64() - cc0);
     } else {
-      ms_apply_cols(sm, buf, H, ld, kb, lo, hi, j1n + 1, n, stage + (size_t)wid * 32 * NR, wid - 1,
-                    NT / 32 - 1, lane);
-      ms_apply_rows(sm, buf, H, Z, ld, n, kb, lo, hi, j0, tid - 32, NT - 32);
+      ms_apply_cols(sm, buf, H, ld, kb, lo, hi, j1n + 1, n, stage + (size_t)wid * 32 * NR, wid - 1, NG, lane);
+      ms_apply_rows(sm, buf, H, Z, ld, n, kb, lo, hi, j0, tid - 32, NG * 32);
       SCHUR_STAT_T(32, 10, clock64() - cc0);
     }
-    __syncthreads();
+    if constexpr (CL > 1)
+      mat_sync<CL>();
+    else
+      __syncthreads();
     SCHUR_STAT(11, clock64() - cc0);
     SCHUR_STAT(12, 1);
   }
+}
+
+// Helper CTA `rank` (>= 1) of a cluster: follows the leader's posted sweeps
+// and applies each chunk's logged reflectors (copied from the leader's
+// shared memory) to its share of the far columns and rows, in lock step with
+// the leader's per-chunk cluster barriers; returns when the leader posts 0.
+// The barrier sequence mirrors multi_sweep<CL> exactly: one after the post,
+// one per chunk; a last one keeps the leader's shared memory alive until
+// every helper has read the final command.
+template <int CL>
+__device__ void schur_helper(Smem& sm, double2* stage, double2* H, double2* Z, int ld, int n, int rank) {
+  constexpr int NG = update_warps<CL>();
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int g = NT / 32 - 1 + (NT / 32) * (rank - 1) + wid;
+  const Smem* L = cooperative_groups::this_cluster().map_shared_rank(&sm, 0);
+  for (;;) {
+    mat_sync<CL>();
+    if (L->cmd != 1) break;
+    const int l = L->cmd_l, i = L->cmd_i;
+    const int T = (i - l) + 2 * (NS - 1);
+    const int C = (T + MW - 1) / MW;
+    for (int c = 0; c < C; ++c) {
+      const int buf = c & 1;
+      for (int e = tid; e < MW * NS; e += NT) {
+        const int st = e / NS, bb = e % NS;
+        sm.rtau[buf][st][bb] = L->rtau[buf][st][bb];
+        sm.rv[buf][st][bb] = L->rv[buf][st][bb];
+      }
+      __syncthreads();
+      const int kb = l + c * MW - 2 * (NS - 1);
+      const int j0 = max(l, kb - 1), j1 = min(i, kb + NR + 1);
+      const int lo = max(l, kb), hi = min(i, kb + NR - 1);
+      const int j1n = (c + 1 < C) ? min(i, kb + MW + NR + 1) : j1;
+      ms_apply_cols(sm, buf, H, ld, kb, lo, hi, j1n + 1, n, stage + (size_t)wid * 32 * NR, g, NG, lane);
+      ms_apply_rows(sm, buf, H, Z, ld, n, kb, lo, hi, j0, g * 32 + lane, NG * 32);
+      mat_sync<CL>();
+    }
+  }
+  mat_sync<CL>();
 }
 
 // ---- aggressive early deflation (zlaqr3 rules) ---------------------------------
@@ -755,13 +836,19 @@ __device__ int aed(Smem& sm, double2* stage, double2* H, double2* Z, int ld, int
   return nd;
 }
 
+// One matrix per CTA (CL = 1), or per cluster of CL CTAs: the leader (rank
+// 0) runs the iteration, helpers share the far updates of its multishift
+// sweeps (schur_helper).
+template <int CL>
 __global__ void __launch_bounds__(NT, 1)
 schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2* __restrict__ Zg,
              double2* __restrict__ lamg, long long slam, uint32_t* __restrict__ status,
              int max_sweeps_per_n) {
   __shared__ Smem sm;
   extern __shared__ double2 stage[];   // [NT/32][32][NR] column staging tiles
-  const int b = blockIdx.x;
+  const int b = blockIdx.x / CL;
+  int rank = 0;
+  if constexpr (CL > 1) rank = (int)cooperative_groups::this_cluster().block_rank();
   double2* H = Hg + (long long)b * stride;
   double2* Z = Zg + (long long)b * stride;
   double2* lam = lamg + (long long)b * slam;
@@ -775,9 +862,21 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
       const int r = (int)(e % n), c = (int)(e / n);
       if (r <= c + 1 && !cfinite(H[(long long)c * ld + r])) bad = 1;
     }
-    if (__syncthreads_or(bad)) {
-      if (tid == 0) atomicOr(status + b, (unsigned)(ST_NONFINITE | ST_EIG_NOCONV));
-      for (int r = tid; r < n; r += NT) lam[r] = cmk(nan(""), nan(""));
+    bad = __syncthreads_or(bad);
+    // every CTA of a cluster has read the untouched H before the leader
+    // changes it, so all of them take the same branch
+    if constexpr (CL > 1) mat_sync<CL>();
+    if (bad) {
+      if (rank == 0) {
+        if (tid == 0) atomicOr(status + b, (unsigned)(ST_NONFINITE | ST_EIG_NOCONV));
+        for (int r = tid; r < n; r += NT) lam[r] = cmk(nan(""), nan(""));
+      }
+      return;
+    }
+  }
+  if constexpr (CL > 1) {
+    if (rank != 0) {
+      schur_helper<CL>(sm, stage, H, Z, ld, n, rank);
       return;
     }
   }
@@ -866,7 +965,7 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
           __syncthreads();
         }
         const long long c1 = clock64();
-        multi_sweep(sm, stage, H, Z, ld, n, l, ib);
+        multi_sweep<CL>(sm, stage, H, Z, ld, n, l, ib);
         SCHUR_STAT(0, 1);
         SCHUR_STAT(2, clock64() - c1);
       } else {
@@ -903,6 +1002,11 @@ schur_kernel(double2* __restrict__ Hg, int ld, long long stride, int n, double2*
     if (tid == 0) atomicOr(status + b, (unsigned)ST_EIG_NOCONV);
     for (int r = tid; r <= i; r += NT) lam[r] = cmk(nan(""), nan(""));
   }
+  if constexpr (CL > 1) {   // release the helpers (schur_helper's last two barriers)
+    if (tid == 0) sm.cmd = 0;
+    mat_sync<CL>();
+    mat_sync<CL>();
+  }
   SCHUR_STAT(6, clock64() - c_start);
   (void)c_start;
 }
@@ -925,19 +1029,113 @@ extern "C" int rcwa_debug_schur_stats(unsigned long long* out, int reset) {
 // caller lowers it (rcwa_eig_set_sweep_cap, host-side fault injection)
 static std::atomic<int> g_sweeps_per_n{100};
 
-int schur_launch(cudaStream_t s, double2* H, int ld, long long sH, int n, double2* Z, double2* lam,
-                 long long slam, uint32_t* status, int batch) {
-  void* tok = prof_begin(s);
-  constexpr size_t stage_bytes = sizeof(double2) * (NT / 32) * 32 * NR;
-  static bool attr_set[64] = {};   // the attribute is per device
+// CTAs per matrix: 0 = chosen per launch (schur_cluster), else forced
+// (rcwa_eig_set_cluster_size: 1, 2, 4 or 8)
+static std::atomic<int> g_cluster_force{0};
+
+namespace {
+
+constexpr size_t kStageBytes = sizeof(double2) * (NT / 32) * 32 * NR;
+constexpr int kClusterMinN = 400;   // below this the chase, not the far updates, bounds a sweep
+
+template <int CL>
+int launch_cl(cudaStream_t s, double2* H, int ld, long long sH, int n, double2* Z, double2* lam, long long slam,
+              uint32_t* status, int batch, int cap) {
+  static bool attr_set[64] = {};   // the attributes are per device
   int dev = 0;
   RCWA_CUDA_TRY(cudaGetDevice(&dev));
   if (dev >= 64 || !attr_set[dev]) {
-    RCWA_CUDA_TRY(cudaFuncSetAttribute(schur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)stage_bytes));
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kStageBytes));
     if (dev < 64) attr_set[dev] = true;
   }
-  schur_kernel<<<batch, NT, stage_bytes, s>>>(H, ld, sH, n, Z, lam, slam, status, g_sweeps_per_n.load());
+  if constexpr (CL == 1) {
+    schur_kernel<1><<<batch, NT, kStageBytes, s>>>(H, ld, sH, n, Z, lam, slam, status, cap);
+  } else {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)batch * CL);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = kStageBytes;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    RCWA_CUDA_TRY(cudaLaunchKernelEx(&cfg, schur_kernel<CL>, H, ld, sH, n, Z, lam, slam, status, cap));
+  }
+  return RCWA_OK;
+}
+
+// Whether clusters of CL of these CTAs (one SM each) can be resident at all
+// on this device (cached per device).
+template <int CL>
+bool cluster_fits() {
+  static int ok[64];   // 0 unknown, 1 yes, 2 no
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+  if (!ok[dev]) {
+    cudaFuncSetAttribute(schur_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CL);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = kStageBytes;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveClusters(&nc, schur_kernel<CL>, &cfg);
+    cudaGetLastError();
+    ok[dev] = (e == cudaSuccess && nc > 0) ? 1 : 2;
+  }
+  return ok[dev] == 1;
+}
+
+// CTAs per matrix: several only for large matrices in launches that leave
+// SMs idle -- the largest power of two (<= 8) with batch * CL <= SMs (a
+// sweep's far updates then run on CL SMs; as many matrices as SMs already
+// fill the device one CTA each).
+int schur_cluster(int n, int batch) {
+  const int f = g_cluster_force.load();
+  if (f > 0) return f;
+  if (n < kClusterMinN) return 1;
+  static int sms[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
+  if (!sms[dev]) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    sms[dev] = v > 0 ? v : 1;
+  }
+  int cl = 1;
+  while (cl < 8 && (long long)batch * (cl * 2) <= sms[dev]) cl *= 2;
+  return cl;
+}
+
+}  // namespace
+
+int schur_launch(cudaStream_t s, double2* H, int ld, long long sH, int n, double2* Z, double2* lam,
+                 long long slam, uint32_t* status, int batch) {
+  void* tok = prof_begin(s);
+  const int cap = g_sweeps_per_n.load();
+  int cl = schur_cluster(n, batch);
+  if (cl >= 8 && !cluster_fits<8>()) cl = 4;
+  if (cl >= 4 && !cluster_fits<4>()) cl = 2;
+  if (cl >= 2 && !cluster_fits<2>()) cl = 1;
+  int rc;
+  switch (cl) {
+    case 8: rc = launch_cl<8>(s, H, ld, sH, n, Z, lam, slam, status, batch, cap); break;
+    case 4: rc = launch_cl<4>(s, H, ld, sH, n, Z, lam, slam, status, batch, cap); break;
+    case 2: rc = launch_cl<2>(s, H, ld, sH, n, Z, lam, slam, status, batch, cap); break;
+    default: rc = launch_cl<1>(s, H, ld, sH, n, Z, lam, slam, status, batch, cap); break;
+  }
+  if (rc) return rc;
   prof_end(s, tok, "schur");
   // work convention: eig with vectors = 100 n^3 real flops per complex matrix,
   // of which Hessenberg (40/3), Q (16/3), triangular vectors (4/3) and the
@@ -950,6 +1148,16 @@ int schur_launch(cudaStream_t s, double2* H, int ld, long long sH, int n, double
 }
 
 }  // namespace rcwa
+
+extern "C" int rcwa_eig_set_cluster_size(int ctas_per_matrix) {
+  if (ctas_per_matrix != 0 && ctas_per_matrix != 1 && ctas_per_matrix != 2 && ctas_per_matrix != 4 &&
+      ctas_per_matrix != 8) {
+    rcwa::set_last_error("ctas_per_matrix must be 0 (automatic), 1, 2, 4 or 8");
+    return RCWA_ERR_INVALID;
+  }
+  rcwa::g_cluster_force.store(ctas_per_matrix);
+  return RCWA_OK;
+}
 
 extern "C" int rcwa_eig_set_sweep_cap(int sweeps_per_n) {
   if (sweeps_per_n < -1) {

@@ -140,6 +140,7 @@ _SIGS = {
     "rcwa_eig": ([_VP, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_eig_noalloc": ([C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_eig_set_sweep_cap": ([C.c_int], C.c_int),
+    "rcwa_eig_set_cluster_size": ([C.c_int], C.c_int),
     "rcwa_debug_gemm_inject_timeout": ([C.c_int], C.c_int),
     "rcwa_lu_solve": ([_VP, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP], C.c_int),
     "rcwa_lu_solve_ex": ([_VP, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP, C.c_int, C.c_int], C.c_int),

@@ -155,6 +155,49 @@ def test_eig_aed_paths(ctx):
     assert np.abs(A[2] @ W[2] - W[2] * lam[2][None, :]).max() < 1e-9 * np.abs(A[2]).max() * n
 
 
+@pytest.mark.parametrize("cl", [2, 4, 8])
+def test_eig_cluster_ctas_match_one_cta(ctx, cl):
+    """The QR iteration with cl CTAs per matrix (a thread-block cluster whose
+    helper CTAs share the far updates of each multishift sweep) applies the
+    same reflectors to the same entries as one CTA: the eigen-decomposition
+    is identical, and a true one."""
+    from rcwa_b200 import lib as L
+    lib = L.load()
+    rng = np.random.default_rng(450 + cl)
+    n = 450
+    A = _rand(rng, 3, n, n)
+    assert lib.rcwa_eig_set_cluster_size(1) == 0
+    try:
+        lam1, W1, st1 = ctx.eig(A)
+        assert lib.rcwa_eig_set_cluster_size(cl) == 0
+        lam2, W2, st2 = ctx.eig(A)
+    finally:
+        lib.rcwa_eig_set_cluster_size(0)
+    assert not st1.any() and not st2.any()
+    assert np.abs(lam2 - lam1).max() <= 1e-13 * np.abs(lam1).max()
+    assert np.abs(W2 - W1).max() <= 1e-12
+    _eig_check(A[0], lam2[0], W2[0])
+    assert lib.rcwa_eig_set_cluster_size(3) == L.RCWA_ERR_INVALID
+
+
+def test_cluster_eigensolver_in_a_solve(ctx):
+    """A single large request (M = 25, n = 1250: few matrices, so the
+    eigensolver runs its QR iteration on clusters of CTAs) gives the same R/T
+    as with one CTA per matrix."""
+    from rcwa_b200 import lib as L
+    lib = L.load()
+    rng = np.random.default_rng(4)
+    pb = C.c3_request(rng, grid=128, m_max=25, m_min=25)
+    a = ctx.solve_sweep(pb)
+    assert lib.rcwa_eig_set_cluster_size(1) == 0
+    try:
+        b = ctx.solve_sweep(pb)
+    finally:
+        lib.rcwa_eig_set_cluster_size(0)
+    assert a[4][0] == 0 and b[4][0] == 0
+    assert np.abs(a[0] - b[0]).max() <= 1e-12 and np.abs(a[1] - b[1]).max() <= 1e-12
+
+
 def test_eig_nonfinite_flagged(ctx):
     A = np.eye(6, dtype=complex)
     A[2, 3] = np.nan
