@@ -47,6 +47,7 @@ namespace {
 
 constexpr int NB = 32;
 constexpr int PANEL_NT = 256;
+constexpr int PANEL_NT_WIDE = 1024;   // large n, few matrices: more rows in flight per column step
 constexpr int COL_NT = 64;
 
 template <class T>
@@ -76,16 +77,16 @@ __device__ __forceinline__ void argmax_reduce(R& v, int& idx) {
   }
 }
 
-template <class T>
-__global__ void __launch_bounds__(PANEL_NT)
+template <class T, int PNT>
+__global__ void __launch_bounds__(PNT)
 lu_panel_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int j, int jb,
                 int* __restrict__ pivg, uint32_t* __restrict__ status) {
   using R = typename Cx<T>::R;
   const int b = blockIdx.x;
   T* M = Mg + (long long)b * stride;
   int* piv = pivg + (long long)b * n;
-  __shared__ R s_val[PANEL_NT / 32];
-  __shared__ int s_idx[PANEL_NT / 32];
+  __shared__ R s_val[PNT / 32];
+  __shared__ int s_idx[PNT / 32];
   __shared__ T s_urow[NB];
   __shared__ int s_p;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -96,7 +97,7 @@ lu_panel_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int j, int 
     // 1. pivot search over rows col..n-1 (|re|+|im|, first maximum wins)
     R best = -1;
     int bi = n;
-    for (int r = col + tid; r < n; r += PANEL_NT) {
+    for (int r = col + tid; r < n; r += PNT) {
       R v = cabs1(Mc[r]);
       if (v > best) { best = v; bi = r; }
     }
@@ -104,8 +105,8 @@ lu_panel_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int j, int 
     if (lane == 0) { s_val[wid] = best; s_idx[wid] = bi; }
     __syncthreads();
     if (wid == 0) {
-      best = lane < PANEL_NT / 32 ? s_val[lane] : R(-1);
-      bi = lane < PANEL_NT / 32 ? s_idx[lane] : n;
+      best = lane < PNT / 32 ? s_val[lane] : R(-1);
+      bi = lane < PNT / 32 ? s_idx[lane] : n;
       argmax_reduce(best, bi);
       if (lane == 0) {
         if (bi >= n) bi = col;
@@ -117,7 +118,7 @@ lu_panel_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int j, int 
     const int p = s_p;
     // 2. swap rows col <-> p inside the panel
     if (p != col) {
-      for (int cc = tid; cc < jb; cc += PANEL_NT) {
+      for (int cc = tid; cc < jb; cc += PNT) {
         T* q = M + (long long)(j + cc) * ld;
         T t = q[col];
         q[col] = q[p];
@@ -126,13 +127,13 @@ lu_panel_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int j, int 
     }
     __syncthreads();
     // 3. pivot row of the remaining panel columns -> smem
-    for (int cc = c + 1 + tid; cc < jb; cc += PANEL_NT) s_urow[cc] = M[(long long)(j + cc) * ld + col];
+    for (int cc = c + 1 + tid; cc < jb; cc += PNT) s_urow[cc] = M[(long long)(j + cc) * ld + col];
     const T pv = Mc[col];
     if (tid == 0 && pv.x == R(0) && pv.y == R(0)) atomicOr(status + b, (unsigned)ST_SINGULAR);
     __syncthreads();
     const T inv = crcp(pv);
     // 4. scale the column below the pivot and rank-1 update the panel
-    for (int r = col + 1 + tid; r < n; r += PANEL_NT) {
+    for (int r = col + 1 + tid; r < n; r += PNT) {
       T l = cmul(Mc[r], inv);
       Mc[r] = l;
       for (int cc = c + 1; cc < jb; ++cc) {
@@ -452,15 +453,33 @@ int perm_attrs() {
   return RCWA_OK;
 }
 
+int panel_sms() {
+  static int sms[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
+  if (!sms[dev]) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    sms[dev] = v > 0 ? v : 1;
+  }
+  return sms[dev];
+}
+
 // 1. P A = L U on the A part of the augmented M, right-looking over the A
 // columns only (piv receives the interchanges).
 template <class T>
 int lu_factor(cudaStream_t s, int n, T* M, int ld, long long stride, int batch, int* piv,
               uint32_t* status) {
+  // the panel is latency-bound (one CTA per matrix, column by column): with
+  // few large matrices, four times the threads per column step
+  const bool wide = n >= 512 && batch < panel_sms();
   for (int j = 0; j < n; j += NB) {
     const int jb = (n - j < NB) ? (n - j) : NB;
     void* tok = prof_begin(s);
-    lu_panel_kernel<T><<<batch, PANEL_NT, 0, s>>>(M, ld, stride, n, j, jb, piv, status);
+    if (wide)
+      lu_panel_kernel<T, PANEL_NT_WIDE><<<batch, PANEL_NT_WIDE, 0, s>>>(M, ld, stride, n, j, jb, piv, status);
+    else
+      lu_panel_kernel<T, PANEL_NT><<<batch, PANEL_NT, 0, s>>>(M, ld, stride, n, j, jb, piv, status);
     prof_end(s, tok, "lu_panel");
     count_launch();
     RCWA_LAUNCH_CHECK();
