@@ -375,11 +375,19 @@ int rcwa_lu_solve_ex(rcwa_context* ctx, int n, int nrhs, int batch, const rcwa_c
  * rcwa.cpp). */
 int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_complex* A,
               const rcwa_complex* B, rcwa_complex* C, int precision);
-/* rcwa_gemm on device arrays (batch-packed, column-major), asynchronous on
- * the context's stream; the mixed-precision GEMM's workspace comes from the
- * context's workspace. */
-int rcwa_gemm_device(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_complex* A_dev,
-                     const rcwa_complex* B_dev, rcwa_complex* C_dev, int precision);
+/* C = alpha A B + beta C on device arrays (batch-packed, column-major),
+ * asynchronous on the context's stream; the mixed-precision GEMM's workspace
+ * comes from the context's workspace. */
+int rcwa_gemm_device(rcwa_context* ctx, int m, int n, int k, int batch, rcwa_complex alpha,
+                     const rcwa_complex* A_dev, const rcwa_complex* B_dev, rcwa_complex beta,
+                     rcwa_complex* C_dev, int precision);
+/* FP64 GEMM kernel per shape bucket (no reference counterpart), usually the
+ * table written by the project's tuner (rcwa_b200/tune.py): choice[5 kb + sb]
+ * for k bucket kb (k <= 16, <= 32, <= 64, <= 128, larger) and size bucket sb
+ * (min(m, n) <= 64, <= 128, <= 256, <= 512, larger); 0 = the FP64 tensor-core
+ * (DMMA) kernel, 1 = the CUDA-core kernel, -1 = the built-in rule (DMMA for
+ * k > 64).  NULL restores the built-in rule.  Process-wide. */
+int rcwa_set_gemm_table(const int* choice);
 /* C = alpha op(A) op(B) + beta C, batched, column-major host arrays; op = 1
  * takes the conjugate transpose (A stored k x m, B stored n x k), C is read
  * when beta != 0.  FP64 only. */

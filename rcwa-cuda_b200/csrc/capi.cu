@@ -560,8 +560,9 @@ int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_comp
   return RCWA_OK;
 }
 
-int rcwa_gemm_device(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_complex* A,
-                     const rcwa_complex* B, rcwa_complex* C, int precision) {
+int rcwa_gemm_device(rcwa_context* ctx, int m, int n, int k, int batch, rcwa_complex alpha,
+                     const rcwa_complex* A, const rcwa_complex* B, rcwa_complex beta, rcwa_complex* C,
+                     int precision) {
   CHECK_ARG(ctx && A && B && C && m > 0 && n > 0 && k > 0 && batch > 0, "bad argument");
   CHECK_ARG(precision == RCWA_PREC_FP64 || precision == RCWA_PREC_MIXED, "unknown precision mode");
   RCWA_CUDA_TRY(cudaSetDevice(ctx->device));
@@ -574,6 +575,8 @@ int rcwa_gemm_device(rcwa_context* ctx, int m, int n, int k, int batch, const rc
   g.A = (const double2*)A; g.lda = m; g.sA = (long long)m * k;
   g.B = (const double2*)B; g.ldb = k; g.sB = (long long)k * n;
   g.C = (double2*)C; g.ldc = m; g.sC = (long long)m * n;
+  g.alpha = make_double2(alpha.re, alpha.im);
+  g.beta = make_double2(beta.re, beta.im);
   g.tc = kind;
   g.digits = ctx->oz_digits;
   g.ws = ctx->ws;

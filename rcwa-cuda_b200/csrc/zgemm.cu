@@ -13,6 +13,7 @@
 // 4x4 complex micro-tile) is kept as the alternative.  Both stage A and B
 // tiles with cp.async (16-byte copies, zero-filled outside the matrix).
 // tcgen05 has no FP64 kind, so FP64 tensor work on sm_100a is mma.sync DMMA.
+#include <atomic>
 #include <cstring>
 
 #include "common.cuh"
@@ -313,14 +314,28 @@ zgemm_dmma_kernel(int m, int n, int k, double2 alpha, const double2* __restrict_
     live_j |= (n0 + wn * 32 + q * 8 < n) ? (1 << q) : 0;
   }
 
+  // C += +-A B (alpha = +-1, no diagonal scalings, beta != 0: the LU and
+  // Hessenberg rank-k updates): the accumulators start from +-beta C, read
+  // before the k loop so that the read overlaps the first tile loads; the
+  // result is then sgn * acc
+  const bool pre = !dl && !dr && (beta.x != 0.0 || beta.y != 0.0) && alpha.y == 0.0 &&
+                   (alpha.x == 1.0 || alpha.x == -1.0);
+  const double sgn = pre ? alpha.x : 1.0;
   double cr[4][4][2], ci[4][4][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      cr[i][j][0] = cr[i][j][1] = 0.0;
-      ci[i][j][0] = ci[i][j][1] = 0.0;
-    }
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        cr[i][j][q] = ci[i][j][q] = 0.0;
+        const int row = m0 + wm * 32 + i * 8 + lr, col = n0 + wn * 32 + j * 8 + lk * 2 + q;
+        if (pre && row < m && col < n) {
+          const double2 c0 = cmul(beta, C[(long long)col * ldc + row]);
+          cr[i][j][q] = sgn * c0.x;
+          ci[i][j][q] = sgn * c0.y;
+        }
+      }
 
   auto load_tile = [&](int buf, int k0) {
 #pragma unroll
@@ -403,6 +418,11 @@ zgemm_dmma_kernel(int m, int n, int k, double2 alpha, const double2* __restrict_
       for (int i = 0; i < 4; ++i) {
         const int row = m0 + wm * 32 + i * 8 + lr;
         if (row >= m) continue;
+        double2* cpre = C + (long long)col * ldc + row;
+        if (pre) {
+          *cpre = cmk(sgn * cr[i][j][q], sgn * ci[i][j][q]);
+          continue;
+        }
         double2 v = cmul(alpha, cmk(cr[i][j][q], ci[i][j][q]));
         if (dl) v = cmul(dl[(long long)b * sdl + row], v);
         if (dr) v = cmul(v, sr);
@@ -426,19 +446,33 @@ int thin_cut(int extent) {
   return (on && extent > 64 && r != 0 && r <= 16) ? r : 0;
 }
 
-// Kernel choice.  Default: the DMMA kernel for k > 64 and the CUDA-core
-// kernel for the rank-k updates (k <= 64) of the LU factorisations -- in the
-// C2 sweep on B200 the DMMA kernel ran the k = 450 GEMMs at 21.8 TFLOP/s
-// (CUDA cores: 16.1) and the rank-32 updates at 9.0 (CUDA cores: 12.0).
-// RCWA_ZGEMM=ffma or =dmma (read once) forces one kernel for every shape.
-int gemm_impl(int k) {
+// Kernel choice per shape bucket: k in (<=16, <=32, <=64, <=128, more) by
+// min(m, n) in (<=64, <=128, <=256, <=512, more); entry 0 = DMMA kernel,
+// 1 = CUDA-core kernel, -1 = the built-in rule (DMMA for k > 64, CUDA cores
+// for the rank-k updates).  A measured table comes from the tuner
+// (rcwa_set_gemm_table); RCWA_ZGEMM=ffma or =dmma (read once) forces one
+// kernel for every shape.
+std::atomic<int> g_gemm_table[25];
+std::atomic<bool> g_gemm_table_init{false};
+
+int gemm_bucket_k(int k) { return k <= 16 ? 0 : k <= 32 ? 1 : k <= 64 ? 2 : k <= 128 ? 3 : 4; }
+int gemm_bucket_mn(int m, int n) {
+  const int s = m < n ? m : n;
+  return s <= 64 ? 0 : s <= 128 ? 1 : s <= 256 ? 2 : s <= 512 ? 3 : 4;
+}
+
+int gemm_impl(int m, int n, int k) {
   static int impl = -1;
   if (impl < 0) {
     const char* e = getenv("RCWA_ZGEMM");
     impl = (e && strcmp(e, "ffma") == 0) ? 1 : (e && strcmp(e, "dmma") == 0) ? 2 : 0;
   }
-  if (impl == 0) return k > 64 ? 0 : 1;
-  return impl == 2 ? 0 : 1;
+  if (impl != 0) return impl == 2 ? 0 : 1;
+  if (g_gemm_table_init.load()) {
+    const int c = g_gemm_table[gemm_bucket_k(k) * 5 + gemm_bucket_mn(m, n)].load();
+    if (c == 0 || c == 1) return c;
+  }
+  return k > 64 ? 0 : 1;
 }
 
 template <int WM, int ST>
@@ -493,7 +527,7 @@ int zgemm(cudaStream_t s, const ZGemm& g) {
 #define RCWA_ZGEMM_ARGS                                                                          \
   g.m, g.n, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
       g.dr, g.sdr
-  if (gemm_impl(kk) == 0) {
+  if (gemm_impl(g.m, g.n, kk) == 0) {
     if ((rc = launch_dmma<2, 4>(s, g, grid, thin_cut(g.m), thin_cut(g.n)))) return rc;
   } else {
     if (g.opA == 0 && g.opB == 0) zgemm_kernel<0, 0, 4><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
@@ -515,3 +549,16 @@ int zgemm(cudaStream_t s, const ZGemm& g) {
 }
 
 }  // namespace rcwa
+
+extern "C" int rcwa_set_gemm_table(const int* choice) {
+  for (int i = 0; i < 25; ++i) {
+    const int c = choice ? choice[i] : -1;
+    if (c < -1 || c > 1) {
+      rcwa::set_last_error("gemm table entries must be -1, 0 or 1");
+      return RCWA_ERR_INVALID;
+    }
+  }
+  for (int i = 0; i < 25; ++i) rcwa::g_gemm_table[i].store(choice ? choice[i] : -1);
+  rcwa::g_gemm_table_init.store(choice != nullptr);
+  return RCWA_OK;
+}

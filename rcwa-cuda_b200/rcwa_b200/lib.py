@@ -147,7 +147,9 @@ _SIGS = {
     "rcwa_gemm_ex": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, CComplex, _VP, _VP,
                       CComplex, _VP], C.c_int),
     "rcwa_gemm": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, C.c_int], C.c_int),
-    "rcwa_gemm_device": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, C.c_int], C.c_int),
+    "rcwa_gemm_device": ([_VP, C.c_int, C.c_int, C.c_int, C.c_int, CComplex, _VP, _VP, CComplex, _VP, C.c_int],
+                         C.c_int),
+    "rcwa_set_gemm_table": ([_VP], C.c_int),
     "rcwa_rasterize": ([_VP, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.POINTER(CLayerShapes),
                         _VP, _VP, _VP], C.c_int),
     "rcwa_geometry_create_shapes": ([_VP, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
@@ -232,14 +234,34 @@ def c_source(s: SourceSpec) -> CSource:
     return CSource(float(s.lambda0), float(s.theta), float(s.phi), float(s.pte), float(s.ptm))
 
 
+_tuning_applied = False
+
+
+def apply_tuning(path: Optional[str] = None) -> bool:
+    """Hands the tuner's GEMM kernel table (rcwa_b200/tune.py) to the
+    library; False when no table has been written.  Done once by the first
+    Context unless RCWA_NO_TUNING=1."""
+    from . import tune
+    ch = tune.load_table(path or tune.TABLE_PATH)
+    if ch is None:
+        return False
+    arr = (C.c_int * 25)(*ch)
+    _check(load().rcwa_set_gemm_table(arr))
+    return True
+
+
 class Context:
     """One CUDA stream + device workspace (``rcwa_context``)."""
 
     def __init__(self, device: int = 0):
+        global _tuning_applied
         self.lib = load()
         h = C.c_void_p()
         _check(self.lib.rcwa_context_create(device, C.byref(h)))
         self.h = h
+        if not _tuning_applied and os.environ.get("RCWA_NO_TUNING") != "1":
+            _tuning_applied = True
+            apply_tuning()
 
     def close(self):
         if self.h:
@@ -484,10 +506,12 @@ class Context:
         Cm = Cf.transpose(0, 2, 1)
         return Cm[0] if single else Cm
 
-    def gemm_device(self, A_ptr, B_ptr, C_ptr, m, n, k, batch, precision: int = PREC_FP64):
-        """``rcwa_gemm_device``: C = A B on batch-packed column-major device
-        arrays, asynchronous on the context's stream."""
-        _check(self.lib.rcwa_gemm_device(self.h, m, n, k, batch, A_ptr, B_ptr, C_ptr, precision))
+    def gemm_device(self, A_ptr, B_ptr, C_ptr, m, n, k, batch, precision: int = PREC_FP64, alpha=1.0, beta=0.0):
+        """``rcwa_gemm_device``: C = alpha A B + beta C on batch-packed
+        column-major device arrays, asynchronous on the context's stream."""
+        a, b = complex(alpha), complex(beta)
+        _check(self.lib.rcwa_gemm_device(self.h, m, n, k, batch, CComplex(a.real, a.imag), A_ptr, B_ptr,
+                                         CComplex(b.real, b.imag), C_ptr, precision))
 
     def gemm_ex(self, A, B, C=None, opa=0, opb=0, alpha=1.0, beta=0.0):
         """``rcwa_gemm_ex``: alpha op(A) op(B) + beta C on [b, rows, cols]
