@@ -248,6 +248,11 @@ void set_gemm_kind(const rcwa_context* ctx, unsigned stage, ZGemm& g) {
     g.tc = TC_TF32;
     return;
   }
+  // the int8-slice kernel pays off on large products only: its 128-row
+  // tiles and split passes are mostly waste below a few hundred rows, where
+  // the FP64 kernel is both faster and exact
+  constexpr int kInt8MinMN = 256;
+  if (g.m < kInt8MinMN || g.n < kInt8MinMN || g.k < kInt8MinMN) return;
   g.tc = TC_INT8;
   g.digits = ctx->oz_digits;
   g.ws = ctx->ozws;

@@ -154,9 +154,10 @@ def _mixed_vs_fp64(ctx, pb, stages=None):
 
 
 def test_mixed_c1_te_tm(ctx):
+    """C1 (n = 98): every product is below the int8-slice kernel's size
+    threshold (256), so the mixed form runs them in FP64 -- the same result."""
     d, r0, r1 = _mixed_vs_fp64(ctx, C.c1_pillars())
-    assert d <= TOL_MIXED, d
-    assert d > 1e-14, d          # the reduced-precision stages really ran
+    assert d <= 1e-13, d
 
 
 def test_mixed_c2_full_sweep(ctx):
