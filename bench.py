@@ -313,20 +313,20 @@ def served_block(count, rates, seed=5):
     the same request list and arrival times for FP64 and mixed precision.
     Per precision and offered rate: served requests/s (completed / span from
     the first submit to the last completion), p50 / p99 submit-to-completion
-    latency, requests refused by back-pressure (queue limit 64); for mixed,
+    latency, requests refused by back-pressure (queue limit 256); for mixed,
     max |dR|, |dT| against the FP64 result of the same request."""
     from rcwa_b200 import lib as L, configs as C
     rng = np.random.default_rng(seed)
     pbs = [C.c3_request(rng, 128, 25) for _ in range(count)]
     out = {"workload": f"{count} C3-distributed requests per rate (odd M 5..25, n <= 1250, 1-6 layers, 128^2 "
-                       "grids), Poisson arrivals, 3 lanes, queue limit 64",
+                       "grids), Poisson arrivals, 2 lanes of up to 128 requests, queue limit 256",
            "rates": []}
     results = {}
     for rate in rates:
         arr = C.poisson_arrivals(rate, count, seed=int(rate))
         row = {"rate_hz": rate}
         for prec_name, prec in (("fp64", L.PREC_FP64), ("mixed", L.PREC_MIXED)):
-            srv = L.Server(0, max_batch=64, max_queue=64, precision=prec)
+            srv = L.Server(0, max_batch=128, max_queue=256, precision=prec, lanes=2)
             try:
                 srv.poll(srv.submit(pbs[0]), pbs[0], wait=True)       # warm-up (plans, pools)
                 t0 = time.perf_counter()

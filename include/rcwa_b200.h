@@ -238,7 +238,7 @@ typedef struct rcwa_server_config {
   int max_batch;              /* requests per batched solve of a lane (> 0) */
   int max_queue;              /* waiting requests before RCWA_ERR_BUSY (> 0) */
   int precision;              /* RCWA_PREC_FP64 or RCWA_PREC_MIXED */
-  int lanes;                  /* concurrent batches, 1..16 (0: 3) */
+  int lanes;                  /* concurrent batches, 1..16 (0: 2) */
   uint64_t hbm_budget_bytes;  /* in-flight footprint limit (0: min(180 GB, 85 % of free memory)) */
   unsigned mixed_stages;      /* as rcwa_context_set_mixed (0: its defaults) */
   int refine_sweeps;

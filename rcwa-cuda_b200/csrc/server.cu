@@ -268,7 +268,7 @@ int rcwa_server_create_ex(int device, const rcwa_server_config* cfg, rcwa_server
   S->max_batch = cfg->max_batch;
   S->max_queue = cfg->max_queue;
   S->precision = cfg->precision;
-  S->nlanes = cfg->lanes ? cfg->lanes : 3;
+  S->nlanes = cfg->lanes ? cfg->lanes : 2;   // measured on the C3-type mix: 2 lanes of large batches serve most
   if (cfg->mixed_stages) S->mixed_stages = cfg->mixed_stages;
   if (cfg->refine_sweeps) S->refine_sweeps = cfg->refine_sweeps;
   if (cfg->gemm_digits) S->gemm_digits = cfg->gemm_digits;
