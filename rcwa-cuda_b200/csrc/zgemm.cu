@@ -24,6 +24,13 @@ namespace rcwa {
 namespace {
 
 constexpr int BM = 64, BN = 64, BK = 8, NT = 256;
+// DMMA kernel shape: WM warps along M (CTA tile 32 WM x 64), ST pipeline stages
+#ifndef RCWA_DMMA_WM
+#define RCWA_DMMA_WM 2
+#endif
+#ifndef RCWA_DMMA_ST
+#define RCWA_DMMA_ST 4
+#endif
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
   unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
@@ -528,7 +535,7 @@ int zgemm(cudaStream_t s, const ZGemm& g) {
   g.m, g.n, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
       g.dr, g.sdr
   if (gemm_impl(g.m, g.n, kk) == 0) {
-    if ((rc = launch_dmma<2, 4>(s, g, grid, thin_cut(g.m), thin_cut(g.n)))) return rc;
+    if ((rc = launch_dmma<RCWA_DMMA_WM, RCWA_DMMA_ST>(s, g, grid, thin_cut(g.m), thin_cut(g.n)))) return rc;
   } else {
     if (g.opA == 0 && g.opB == 0) zgemm_kernel<0, 0, 4><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
     else if (g.opA == 1 && g.opB == 0) zgemm_kernel<1, 0, 4><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);

@@ -34,7 +34,8 @@
 // Pipeline (per CTA, 128 threads, 128 x TN complex tile): thread 0 issues the
 // bulk copies (cp.async.bulk with mbarrier complete_tx) of ST stages ahead and
 // the MMAs of each k-step, committing each stage's MMAs to its "empty"
-// mbarrier before the stage is refilled; all four warps then read the
+// mbarrier; the stage of k-step kt-1 is refilled right after k-step kt's
+// MMAs are issued, so the tensor pipe never drains between k-steps; all four warps then read the
 // accumulators out of tensor memory (tcgen05.ld, warp w owns lanes 32w..32w+31)
 // for the epilogue.  Every mbarrier wait is bounded; on time-out the CTA
 // sets the error flag, waits (bounded) for its own copies and MMAs, frees its
@@ -332,12 +333,6 @@ oz_gemm_kernel(int m, int n, int k, int MB, int NB, int KB, double2 alpha, const
     constexpr uint32_t IDESC = oz_idesc<TN>();
     for (int kt = 0; kt < KB && ok; ++kt) {
       const int st = kt % ST;
-      // refill the stage that k-step kt-1 used, once its MMAs are done
-      if (kt >= 1 && kt - 1 + ST < KB) {
-        const int ps = (kt - 1) % ST;
-        if (!mbar_wait(&empty[ps], (uint32_t)(((kt - 1) / ST) & 1))) { ok = false; break; }
-        load(kt - 1 + ST);
-      }
       if (!mbar_wait(&full[st], (uint32_t)((kt / ST) & 1))) { ok = false; break; }
       pending[st] = -1;
       asm volatile("tcgen05.fence::after_thread_sync;");
@@ -362,6 +357,13 @@ oz_gemm_kernel(int m, int n, int k, int MB, int NB, int KB, double2 alpha, const
         }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
           su32(&empty[st])));
+      // refill the stage that k-step kt-1 used once its MMAs are done: they
+      // ran ahead of k-step kt's, which keep the tensor pipe busy meanwhile
+      if (kt >= 1 && kt - 1 + ST < KB) {
+        const int ps = (kt - 1) % ST;
+        if (!mbar_wait(&empty[ps], (uint32_t)(((kt - 1) / ST) & 1))) { ok = false; break; }
+        load(kt - 1 + ST);
+      }
     }
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(&done)));
     if (!ok) {
