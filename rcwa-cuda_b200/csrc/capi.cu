@@ -546,7 +546,13 @@ int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_comp
   g.digits = ctx->oz_digits;
   g.ws = (char*)ctx->ws + base;
   g.ws_bytes = wsb;
-  int* terr = g.tc ? tc_error_flag() : nullptr;
+  // the tensor-core kernels of both precisions (the int8 / TF32 ones and the
+  // TMA-fed FP64 one) set this flag when a bounded barrier wait runs out
+  int* terr = tc_error_flag();
+  if (g.tc && !terr) {
+    set_last_error("tensor-core GEMM: device flag unavailable");
+    return RCWA_ERR_CUDA;
+  }
   if (terr) RCWA_CUDA_TRY(cudaMemsetAsync(terr, 0, sizeof(int), s));
   if ((rc = zgemm(s, g))) return rc;
   RCWA_CUDA_TRY(cudaMemcpyAsync(C, dC, nc * batch * 16, cudaMemcpyDeviceToHost, s));
@@ -554,7 +560,7 @@ int rcwa_gemm(rcwa_context* ctx, int m, int n, int k, int batch, const rcwa_comp
   if (terr) RCWA_CUDA_TRY(cudaMemcpyAsync(&herr, terr, sizeof(int), cudaMemcpyDeviceToHost, s));
   RCWA_CUDA_TRY(cudaStreamSynchronize(s));
   if (herr) {
-    set_last_error("tensor-core GEMM: a bounded wait on the MMA barrier expired");
+    set_last_error("tensor-core GEMM: a bounded wait on a tile barrier expired");
     return RCWA_ERR_CUDA;
   }
   return RCWA_OK;

@@ -53,6 +53,7 @@ int zgemm_tc(cudaStream_t s, const ZGemm& g, int* err);
 size_t zgemm_oz_ws_bytes(int m, int n, int k, int batch, int digits);
 int zgemm_oz(cudaStream_t s, const ZGemm& g, int* err);
 int* tc_error_flag();   // device flag of the current device (set-up once per device)
+int gemm_inject_timeout();   // test hook state (rcwa_debug_gemm_inject_timeout)
 
 // X = A^-1 B on the augmented [A | B] (n x (n+nrhs), column-major, ld >= n),
 // all in FP64; the A part receives the LU factors.

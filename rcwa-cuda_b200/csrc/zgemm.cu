@@ -15,6 +15,10 @@
 // tcgen05 has no FP64 kind, so FP64 tensor work on sm_100a is mma.sync DMMA.
 #include <atomic>
 #include <cstring>
+#include <mutex>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -30,6 +34,9 @@ constexpr int BM = 64, BN = 64, BK = 8, NT = 256;
 #endif
 #ifndef RCWA_DMMA_ST
 #define RCWA_DMMA_ST 4
+#endif
+#ifndef RCWA_DMMA_TMA_ST
+#define RCWA_DMMA_TMA_ST 4
 #endif
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
@@ -440,6 +447,280 @@ zgemm_dmma_kernel(int m, int n, int k, double2 alpha, const double2* __restrict_
     }
 }
 
+// ---------------------------------------------------------------------------
+// TMA-fed DMMA kernel (C = A B with both operands as stored, the form of
+// every S-matrix product and of the LU / Hessenberg rank-k updates).  Same
+// warp tiling and DMMA sequence as zgemm_dmma_kernel; the operand tiles come
+// from the tensor memory accelerator (cp.async.bulk.tensor.3d, 128-byte
+// swizzle, zero fill outside the matrix) into an ST-stage ring guarded by
+// mbarriers: "full" completes when a stage's bytes have landed, "empty" when
+// every warp has read it.  Lane 0 of each warp issues its share of every
+// stage (A boxes g = warp, warp + NW, ...; a 64 / NW-column slice of B): the
+// first ST stages up front, then, after the warp's k-tile t, the refill of
+// the stage of k-tile t-1 once every warp has released it.  No CTA-wide
+// barrier sits in the k loop and the copy issue is spread over the warps.
+//
+// Stage layout (k-tile of BK = 8):
+//   A: TM / 8 boxes of 8 rows x 8 k, 1 KB each; box row kk (one k) is 128
+//      bytes = 8 complex rows, its 16-byte chunk r stored at chunk r ^ kk;
+//   B: 64 columns x 8 k, column c is a 128-byte row, chunk kk at kk ^ (c & 7).
+// A DMMA k-step kq (0, 1) takes k = 2 lk + kq for lane k-index lk: the eight
+// lanes of a quarter warp (two rows or columns x four k) then read eight
+// distinct 16-byte chunks, free of bank conflicts.  The permutation of k is
+// the same for A and B, so the products sum the same terms.
+//
+// Every mbarrier wait is bounded (about a second); if one runs out, each
+// warp waits (bounded) for its copies still in flight, the CTA sets the
+// device error flag and writes NaN over its tile of C, so both precisions
+// report the failure (error flag, non-finite status) and the context stays
+// usable.
+// ---------------------------------------------------------------------------
+constexpr long long DMMA_WAIT_CYCLES = 2000000000LL;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init_n(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive1(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    if (ok) return true;
+    if (clock64() - t0 > DMMA_WAIT_CYCLES) return false;
+  }
+}
+// one box of a 3-D tensor map (x innermost, in FP64 elements) into shared memory
+__device__ __forceinline__ void tma_load3(void* sdst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(sdst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <int WM, int ST>
+struct TmaCfg {
+  static constexpr int TM = 32 * WM, NW = 2 * WM;
+  static constexpr int A_BYTES = TM * BK * 16, B_BYTES = BN * BK * 16, STAGE = A_BYTES + B_BYTES;
+  static constexpr int B_COLS = BN / NW;            // B columns per warp's copy
+  static constexpr int SMEM = ST * STAGE + 1024;   // + slack to align the ring to 1024 bytes
+};
+
+// tmA: (2 m doubles, k, batch or 1) with box (16, 8, 1); tmB: (2 k doubles,
+// n, batch or 1) with box (16, 64 / NW, 1); za / zb: 1 when the operand has
+// a batch stride (else every item reads z = 0).
+template <int WM, int ST>
+__global__ void __launch_bounds__(64 * WM, (WM > 2 ? 1 : 2))
+zgemm_dmma_tma_kernel(int m, int n, int k, double2 alpha, const __grid_constant__ CUtensorMap tmA,
+                      const __grid_constant__ CUtensorMap tmB, int za, int zb,
+                      const double2* __restrict__ A, int lda, long long sA, const double2* __restrict__ B,
+                      int ldb, long long sB, double2 beta, double2* __restrict__ C, int ldc, long long sC,
+                      const double2* __restrict__ dl, long long sdl, const double2* __restrict__ dr,
+                      long long sdr, int mf, int nf, int thin_rows, int* __restrict__ err,
+                      int skip_first_copy) {
+  using Cfg = TmaCfg<WM, ST>;
+  constexpr int TM = Cfg::TM, NW = Cfg::NW;
+  extern __shared__ __align__(16) uint8_t dsm_raw[];
+  __shared__ __align__(8) uint64_t full[ST], empty[ST];
+  uint8_t* ring = (uint8_t*)(((uintptr_t)dsm_raw + 1023) & ~(uintptr_t)1023);
+  const int b = blockIdx.z;
+  A += (long long)b * sA;
+  B += (long long)b * sB;
+  C += (long long)b * sC;
+  if ((int)blockIdx.y < thin_rows) {   // thin-strip CTA, as in zgemm_dmma_kernel
+    const int t = blockIdx.y * gridDim.x + blockIdx.x;
+    const int nrow = mf > m ? (nf + 63) / 64 : 0, ncol = nf > n ? (m + 63) / 64 : 0;
+    const double2* dlb = dl ? dl + (long long)b * sdl : nullptr;
+    const double2* drb = dr ? dr + (long long)b * sdr : nullptr;
+    double2* scratch = reinterpret_cast<double2*>(ring);
+    if (t < nrow)
+      thin_tile<0, 0, 1, 64 * WM>(m, mf, t * 64, min(nf, t * 64 + 64), k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                  dlb, drb, scratch);
+    else if (t < nrow + ncol)
+      thin_tile<0, 0, 0, 64 * WM>((t - nrow) * 64, min(m, (t - nrow) * 64 + 64), n, nf, k, alpha, A, lda, B,
+                                  ldb, beta, C, ldc, dlb, drb, scratch);
+    return;
+  }
+  const int m0 = (blockIdx.y - thin_rows) * TM, n0 = blockIdx.x * BN;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp % WM, wn = warp / WM;
+  const int lr = lane >> 2, lk = lane & 3;
+  int live_i = 0, live_j = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    live_i |= (m0 + wm * 32 + q * 8 < m) ? (1 << q) : 0;
+    live_j |= (n0 + wn * 32 + q * 8 < n) ? (1 << q) : 0;
+  }
+  // A boxes (8-row groups) of this tile that hold any row < m; this warp
+  // copies boxes warp, warp + NW, ... of them and its slice of B
+  const int nbox = min(TM / 8, (m - m0 + 7) / 8);
+  // (boxes wholly outside the matrix are not copied: the DMMAs of their
+  // 8 x 8 blocks are skipped through live_i / live_j)
+  const int my_boxes = nbox > warp ? (nbox - warp + NW - 1) / NW : 0;
+  const bool my_b = n0 + warp * Cfg::B_COLS < n;
+  const uint32_t warp_tx = (uint32_t)(my_boxes * 1024 + (my_b ? Cfg::B_BYTES / NW : 0));
+  const int ktiles = (k + BK - 1) / BK;
+  const int az = za ? b : 0, bzc = zb ? b : 0;
+
+  if (tid == 0) {
+    for (int st = 0; st < ST; ++st) {
+      mbar_init_n(&full[st], NW);
+      mbar_init_n(&empty[st], NW);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  __syncthreads();
+
+  int pending[ST];   // lane 0: per stage, the k-tile whose copies are in flight and not yet waited for, or -1
+#pragma unroll
+  for (int st = 0; st < ST; ++st) pending[st] = -1;
+  auto issue = [&](int t) {   // lane 0 only
+    const int st = t % ST;
+    if (t == 0 && skip_first_copy) return;   // test hook: k-tile 0 never arrives
+    uint8_t* sa = ring + st * Cfg::STAGE;
+    mbar_expect_tx(&full[st], warp_tx);
+    for (int g = warp; g < nbox; g += NW) tma_load3(sa + g * 1024, &tmA, 2 * (m0 + 8 * g), t * BK, az, &full[st]);
+    if (my_b)
+      tma_load3(sa + Cfg::A_BYTES + warp * Cfg::B_COLS * 128, &tmB, 2 * t * BK, n0 + warp * Cfg::B_COLS, bzc,
+                &full[st]);
+    pending[st] = t;
+  };
+  if (lane == 0)
+    for (int p = 0; p < ST && p < ktiles; ++p) issue(p);
+
+  // C += +-A B: accumulators start from +-beta C (as in zgemm_dmma_kernel)
+  const bool pre = !dl && !dr && (beta.x != 0.0 || beta.y != 0.0) && alpha.y == 0.0 &&
+                   (alpha.x == 1.0 || alpha.x == -1.0);
+  const double sgn = pre ? alpha.x : 1.0;
+  double cr[4][4][2], ci[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        cr[i][j][q] = ci[i][j][q] = 0.0;
+        const int row = m0 + wm * 32 + i * 8 + lr, col = n0 + wn * 32 + j * 8 + lk * 2 + q;
+        if (pre && row < m && col < n) {
+          const double2 c0 = cmul(beta, C[(long long)col * ldc + row]);
+          cr[i][j][q] = sgn * c0.x;
+          ci[i][j][q] = sgn * c0.y;
+        }
+      }
+
+  bool ok = true;
+  for (int t = 0; t < ktiles; ++t) {
+    const int st = t % ST;
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[st], (uint32_t)((t / ST) & 1)))) {
+      ok = false;
+      break;
+    }
+    if (lane == 0) pending[st] = -1;
+    const uint8_t* sa = ring + st * Cfg::STAGE;
+    const uint8_t* sb = sa + Cfg::A_BYTES;
+#pragma unroll
+    for (int kq = 0; kq < BK / 4; ++kq) {
+      const int kk = 2 * lk + kq;
+      double ar[4], ai[4], nai[4], br[4], bi[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const double2 v =
+            *reinterpret_cast<const double2*>(sa + (wm * 4 + i) * 1024 + kk * 128 + ((lr ^ kk) << 4));
+        ar[i] = v.x;
+        ai[i] = v.y;
+        nai[i] = -v.y;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double2 v = *reinterpret_cast<const double2*>(sb + (wn * 32 + j * 8 + lr) * 128 + ((kk ^ lr) << 4));
+        br[j] = v.x;
+        bi[j] = v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (!((live_i >> i) & (live_j >> j) & 1)) continue;
+          dmma(cr[i][j], ar[i], br[j]);
+          dmma(cr[i][j], nai[i], bi[j]);
+          dmma(ci[i][j], ar[i], bi[j]);
+          dmma(ci[i][j], ai[i], br[j]);
+        }
+    }
+    __syncwarp();
+    bool pok = true;
+    if (lane == 0) {
+      mbar_arrive1(&empty[st]);
+      if (t >= 1 && t - 1 + ST < ktiles) {
+        if (mbar_wait_bounded(&empty[(t - 1) % ST], (uint32_t)(((t - 1) / ST) & 1))) issue(t - 1 + ST);
+        else pok = false;
+      }
+    }
+    if (!__shfl_sync(0xffffffffu, (int)pok, 0)) {
+      ok = false;
+      break;
+    }
+  }
+  ok = __syncthreads_and(ok);
+  if (!ok) {
+    if (lane == 0) {
+      for (int st = 0; st < ST; ++st)
+        if (pending[st] >= 0) mbar_wait_bounded(&full[st], (uint32_t)((pending[st] / ST) & 1));
+      if (warp == 0) atomicOr(err, 1);
+    }
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int row = m0 + wm * 32 + i * 8 + lr, col = n0 + wn * 32 + j * 8 + lk * 2 + q;
+          if (row < m && col < n) C[(long long)col * ldc + row] = cmk(nan, nan);
+        }
+    return;
+  }
+
+  const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int col = n0 + wn * 32 + j * 8 + lk * 2 + q;
+      if (col >= n) continue;
+      const double2 sr = dr ? dr[(long long)b * sdr + col] : cmk(1.0, 0.0);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int row = m0 + wm * 32 + i * 8 + lr;
+        if (row >= m) continue;
+        double2* cp = C + (long long)col * ldc + row;
+        if (pre) {
+          *cp = cmk(sgn * cr[i][j][q], sgn * ci[i][j][q]);
+          continue;
+        }
+        double2 v = cmul(alpha, cmk(cr[i][j][q], ci[i][j][q]));
+        if (dl) v = cmul(dl[(long long)b * sdl + row], v);
+        if (dr) v = cmul(v, sr);
+        if (use_beta) v = cadd(v, cmul(beta, *cp));
+        *cp = v;
+      }
+    }
+}
+
 // Rows / columns past the last multiple of 64 that go to thin-strip CTAs
 // (0: the tensor-core tiles cover them).  RCWA_ZGEMM_THIN=0 (read once)
 // keeps whole 64-wide tiles everywhere.
@@ -454,11 +735,12 @@ int thin_cut(int extent) {
 }
 
 // Kernel choice per shape bucket: k in (<=16, <=32, <=64, <=128, more) by
-// min(m, n) in (<=64, <=128, <=256, <=512, more); entry 0 = DMMA kernel,
-// 1 = CUDA-core kernel, -1 = the built-in rule (DMMA for k > 64, CUDA cores
-// for the rank-k updates).  A measured table comes from the tuner
-// (rcwa_set_gemm_table); RCWA_ZGEMM=ffma or =dmma (read once) forces one
-// kernel for every shape.
+// min(m, n) in (<=64, <=128, <=256, <=512, more); entry 0 = DMMA kernel fed
+// by cp.async, 1 = CUDA-core kernel, 2 = DMMA kernel fed by TMA (products
+// with both operands as stored; the others take entry 0's kernel), -1 = the
+// built-in rule (DMMA for k > 64, CUDA cores for the rank-k updates).  A
+// measured table comes from the tuner (rcwa_set_gemm_table); RCWA_ZGEMM=ffma,
+// =dmma or =tma (read once) forces one kernel for every shape.
 std::atomic<int> g_gemm_table[25];
 std::atomic<bool> g_gemm_table_init{false};
 
@@ -469,21 +751,88 @@ int gemm_bucket_mn(int m, int n) {
 }
 
 int gemm_impl(int m, int n, int k) {
-  static int impl = -1;
-  if (impl < 0) {
+  static int forced = -2;
+  if (forced == -2) {
     const char* e = getenv("RCWA_ZGEMM");
-    impl = (e && strcmp(e, "ffma") == 0) ? 1 : (e && strcmp(e, "dmma") == 0) ? 2 : 0;
+    forced = !e ? -1 : strcmp(e, "ffma") == 0 ? 1 : strcmp(e, "dmma") == 0 ? 0 : strcmp(e, "tma") == 0 ? 2 : -1;
   }
-  if (impl != 0) return impl == 2 ? 0 : 1;
+  if (forced >= 0) return forced;
   if (g_gemm_table_init.load()) {
     const int c = g_gemm_table[gemm_bucket_k(k) * 5 + gemm_bucket_mn(m, n)].load();
-    if (c == 0 || c == 1) return c;
+    if (c >= 0 && c <= 2) return c;
   }
   return k > 64 ? 0 : 1;
 }
 
+// cuTensorMapEncodeTiled from the driver, through the runtime's entry-point
+// query (the library links only the runtime); null when unavailable.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// 3-D FP64 tensor map (d0 innermost) with a (b0, b1, 1) box and the 128-byte
+// swizzle; false when the driver rejects it (the caller then uses cp.async).
+bool make_tensor_map(CUtensorMap* map, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t s1,
+                     uint64_t s2, uint32_t b0, uint32_t b1) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || ((uintptr_t)base & 15) || (s1 & 15) || (s2 & 15) || s1 >= (1ull << 40) || s2 >= (1ull << 40))
+    return false;
+  const cuuint64_t dims[3] = {d0, d1, d2};
+  const cuuint64_t strides[2] = {s1, s2};
+  const cuuint32_t box[3] = {b0, b1, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(base), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Launches the TMA-fed kernel; *launched stays false (nothing queued) when a
+// tensor map cannot be made or the device flag is unavailable.
 template <int WM, int ST>
-int launch_dmma(cudaStream_t s, const ZGemm& g, dim3 grid, int cm = 0, int cn = 0) {
+int launch_dmma_tma(cudaStream_t s, const ZGemm& g, dim3 grid, int mm, int nm, int kk, int thin_rows,
+                    bool* launched) {
+  using Cfg = TmaCfg<WM, ST>;
+  *launched = false;
+  int* err = tc_error_flag();
+  if (!err) return RCWA_OK;
+  const bool za = g.batch > 1 && g.sA != 0, zb = g.batch > 1 && g.sB != 0;
+  const uint64_t k1 = kk > 0 ? (uint64_t)kk : 1;
+  alignas(64) CUtensorMap tmA, tmB;
+  if (!make_tensor_map(&tmA, g.A, 2ull * mm, k1, za ? (uint64_t)g.batch : 1, (uint64_t)g.lda * 16,
+                       za ? (uint64_t)g.sA * 16 : (uint64_t)g.lda * 16 * k1, 16, BK))
+    return RCWA_OK;
+  if (!make_tensor_map(&tmB, g.B, 2 * k1, (uint64_t)nm, zb ? (uint64_t)g.batch : 1, (uint64_t)g.ldb * 16,
+                       zb ? (uint64_t)g.sB * 16 : (uint64_t)g.ldb * 16 * nm, 2 * BK, Cfg::B_COLS))
+    return RCWA_OK;
+  static bool attr[64] = {};   // per device
+  int dev = 0;
+  RCWA_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 64 || !attr[dev]) {
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(zgemm_dmma_tma_kernel<WM, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       Cfg::SMEM));
+    if (dev < 64) attr[dev] = true;
+  }
+  zgemm_dmma_tma_kernel<WM, ST><<<grid, 64 * WM, Cfg::SMEM, s>>>(
+      mm, nm, kk, g.alpha, tmA, tmB, za ? 1 : 0, zb ? 1 : 0, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C,
+      g.ldc, g.sC, g.dl, g.sdl, g.dr, g.sdr, g.m, g.n, thin_rows, err, gemm_inject_timeout() ? 1 : 0);
+  *launched = true;
+  return RCWA_OK;
+}
+
+template <int WM, int ST>
+int launch_dmma(cudaStream_t s, const ZGemm& g, dim3 grid, int cm = 0, int cn = 0, bool tma = false) {
   constexpr int smem = ST * BK * (32 * WM + 2 + BN + 2) * (int)sizeof(double2);
   static bool attr[64] = {};   // per device
   int dev = 0;
@@ -503,6 +852,11 @@ int launch_dmma(cudaStream_t s, const ZGemm& g, dim3 grid, int cm = 0, int cn = 
   const int thin_rows = cdiv_up(thin, (int)grid.x);
   grid.y = cdiv_up(mm, 32 * WM) + thin_rows;
   const int kk = g.k < 0 ? 0 : g.k;
+  if (tma && g.opA == 0 && g.opB == 0) {
+    bool launched = false;
+    const int rc = launch_dmma_tma<WM, RCWA_DMMA_TMA_ST>(s, g, grid, mm, nm, kk, thin_rows, &launched);
+    if (rc || launched) return rc;
+  }
 #define RCWA_DMMA_ARGS                                                                           \
   mm, nm, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
       g.dr, g.sdr, g.m, g.n, thin_rows
@@ -534,8 +888,10 @@ int zgemm(cudaStream_t s, const ZGemm& g) {
 #define RCWA_ZGEMM_ARGS                                                                          \
   g.m, g.n, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
       g.dr, g.sdr
-  if (gemm_impl(g.m, g.n, kk) == 0) {
-    if ((rc = launch_dmma<RCWA_DMMA_WM, RCWA_DMMA_ST>(s, g, grid, thin_cut(g.m), thin_cut(g.n)))) return rc;
+  const int impl = gemm_impl(g.m, g.n, kk);
+  if (impl != 1) {
+    if ((rc = launch_dmma<RCWA_DMMA_WM, RCWA_DMMA_ST>(s, g, grid, thin_cut(g.m), thin_cut(g.n), impl == 2)))
+      return rc;
   } else {
     if (g.opA == 0 && g.opB == 0) zgemm_kernel<0, 0, 4><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
     else if (g.opA == 1 && g.opB == 0) zgemm_kernel<1, 0, 4><<<grid, NT, 0, s>>>(RCWA_ZGEMM_ARGS);
@@ -560,8 +916,8 @@ int zgemm(cudaStream_t s, const ZGemm& g) {
 extern "C" int rcwa_set_gemm_table(const int* choice) {
   for (int i = 0; i < 25; ++i) {
     const int c = choice ? choice[i] : -1;
-    if (c < -1 || c > 1) {
-      rcwa::set_last_error("gemm table entries must be -1, 0 or 1");
+    if (c < -1 || c > 2) {
+      rcwa::set_last_error("gemm table entries must be -1, 0, 1 or 2");
       return RCWA_ERR_INVALID;
     }
   }

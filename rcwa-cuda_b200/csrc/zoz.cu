@@ -556,6 +556,8 @@ int zgemm_oz(cudaStream_t s, const ZGemm& g, int* err) {
   }
 }
 
+int gemm_inject_timeout() { return g_inject_timeout.load(); }
+
 }  // namespace rcwa
 
 extern "C" int rcwa_debug_gemm_inject_timeout(int on) {

@@ -6,12 +6,13 @@ kernel table the library uses (``rcwa_set_gemm_table``).
 The solve path multiplies matrices of very different shapes: rank-32 updates
 of the blocked LU and Hessenberg reductions (k = 32), the recursive
 triangular solves (k up to n / 2) and the S-matrix algebra (k = n), for n
-from 50 to 2000.  Two FP64 kernels compete: the FP64 tensor-core (DMMA)
-kernel and the CUDA-core kernel.  For every bucket -- k in (<= 16, <= 32,
+from 50 to 2000.  Three FP64 kernels compete: the FP64 tensor-core (DMMA)
+kernel with cp.async tile loads, the same DMMA kernel fed by the tensor
+memory accelerator (TMA) through an mbarrier ring, and the CUDA-core kernel.  For every bucket -- k in (<= 16, <= 32,
 <= 64, <= 128, larger) by min(m, n) in (<= 64, <= 128, <= 256, <= 512,
 larger) -- the tuner times both kernels on a representative square shape,
 in both forms the solver issues (C = A B and the update C = C - A B), with a
-batch that gives each launch a few GFLOP, and keeps the faster one.  The
+batch that gives each launch a few GFLOP, and keeps the fastest.  The
 table is written next to this file (``gemm_tuning_b200.json``); the Python
 binding applies it when the first context is created.
 """
@@ -32,7 +33,7 @@ SIZE_LIMITS = ["mn<=64", "mn<=128", "mn<=256", "mn<=512", "mn>512"]
 
 def _time_kernel(ctx, lib, torch, stream, choice, s, k, batch, reps=5):
     """Median ms of C = A B plus C = C - A B with every bucket forced to
-    `choice` (0 = DMMA, 1 = CUDA cores)."""
+    `choice` (0 = DMMA with cp.async, 1 = CUDA cores, 2 = DMMA fed by TMA)."""
     import ctypes as C
     arr = (C.c_int * 25)(*([choice] * 25))
     assert lib.rcwa_set_gemm_table(arr) == 0
@@ -67,21 +68,21 @@ def tune(path: str = TABLE_PATH) -> dict:
             for s in SIZE_BUCKETS:
                 flops = 2 * 8.0 * s * s * k
                 batch = int(max(1, min(4096, 4e9 / flops)))
-                t_dmma = _time_kernel(ctx, lib, torch, stream, 0, s, k, batch)
-                t_ffma = _time_kernel(ctx, lib, torch, stream, 1, s, k, batch)
-                choice = 0 if t_dmma <= t_ffma else 1
+                t = [_time_kernel(ctx, lib, torch, stream, c, s, k, batch) for c in (0, 1, 2)]
+                choice = min(range(3), key=lambda c: t[c])
                 table.append(choice)
                 rows.append({"k": k, "m=n": s, "batch": batch,
-                             "dmma_tflops": flops * batch / (t_dmma / 1e3) / 1e12,
-                             "cuda_core_tflops": flops * batch / (t_ffma / 1e3) / 1e12,
-                             "choice": "dmma" if choice == 0 else "cuda_core"})
+                             "dmma_tflops": flops * batch / (t[0] / 1e3) / 1e12,
+                             "cuda_core_tflops": flops * batch / (t[1] / 1e3) / 1e12,
+                             "dmma_tma_tflops": flops * batch / (t[2] / 1e3) / 1e12,
+                             "choice": ("dmma", "cuda_core", "dmma_tma")[choice]})
     finally:
         lib.rcwa_set_gemm_table(None)
         ctx.close()
     out = {"device": torch.cuda.get_device_name(0), "date": time.strftime("%Y-%m-%d"),
            "k_buckets": K_LIMITS, "size_buckets": SIZE_LIMITS,
            "choice": table, "measurements": rows,
-           "note": "choice[5 * k_bucket + size_bucket]: 0 = FP64 tensor-core (DMMA) kernel, 1 = CUDA-core kernel"}
+           "note": "choice[5 * k_bucket + size_bucket]: 0 = FP64 tensor-core (DMMA) kernel fed by cp.async, 1 = CUDA-core kernel, 2 = DMMA kernel fed by TMA"}
     with open(path, "w") as f:
         json.dump(out, f, indent=1)
     return out
@@ -94,7 +95,7 @@ def load_table(path: str = TABLE_PATH):
     with open(path) as f:
         t = json.load(f)
     ch = t.get("choice")
-    if not isinstance(ch, list) or len(ch) != 25 or any(c not in (-1, 0, 1) for c in ch):
+    if not isinstance(ch, list) or len(ch) != 25 or any(c not in (-1, 0, 1, 2) for c in ch):
         return None
     return ch
 

@@ -2,10 +2,11 @@
 
 The reference abort()s when its eigensolver does not converge (rcwa.cpp:300);
 here every bounded loop ends with a status the host reads, and the context
-stays usable.  Both failures are made on the host: a QR sweep cap of zero set
+stays usable.  The failures are made on the host: a QR sweep cap of zero set
 by rcwa_eig_set_sweep_cap, and a test hook that leaves out the first operand
-copy of the int8-slice tensor-core GEMM so that its bounded mbarrier wait
-(about a second) runs out.  Nothing here traps, faults or hangs a GPU.
+copy of the int8-slice tensor-core GEMM and of the TMA-fed FP64 GEMM so that
+their bounded mbarrier waits (about a second) run out.  Nothing here traps,
+faults or hangs a GPU.
 """
 import numpy as np
 import pytest
@@ -67,3 +68,30 @@ def test_int8_gemm_wait_timeout_is_reported(ctx):
     got = ctx.gemm(A, B, precision=L.PREC_MIXED)
     ref = A @ B
     assert np.abs(got - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_tma_dmma_gemm_wait_timeout_is_reported(ctx):
+    """The FP64 kernel fed by the tensor memory accelerator: with its first
+    k-tile copy left out, every warp's bounded wait runs out; the call
+    reports the device flag, and the next product is exact again."""
+    import ctypes
+    from rcwa_b200 import lib as L
+    lib = L.load()
+    rng = np.random.default_rng(11)
+    A, B = _rand(rng, 2, 100, 100), _rand(rng, 2, 100, 90)
+    assert lib.rcwa_set_gemm_table((ctypes.c_int * 25)(*([2] * 25))) == L.RCWA_OK
+    try:
+        assert lib.rcwa_debug_gemm_inject_timeout(1) == L.RCWA_OK
+        try:
+            with pytest.raises(L.RcwaError) as e:
+                ctx.gemm(A, B)
+            assert e.value.code == L.RCWA_ERR_CUDA
+            assert "wait" in str(e.value)
+        finally:
+            lib.rcwa_debug_gemm_inject_timeout(0)
+        got = ctx.gemm(A, B)
+        ref = A @ B
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    finally:
+        if not L.apply_tuning():
+            lib.rcwa_set_gemm_table(None)
