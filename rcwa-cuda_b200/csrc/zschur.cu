@@ -47,6 +47,7 @@ constexpr int NS = 8;                        // bulges per multishift sweep
 constexpr int MW = 8;                        // chase steps per chunk
 constexpr int NR = MW + 2 * (NS - 1) + 1;    // rows/cols a chunk's reflectors touch
 constexpr int MWIN = NR + 3;
+static_assert(MWIN <= 32, "the chase warp moves a window row per lane");
 constexpr int MS_MIN = 3 * NS;
 constexpr int WINMAX = MWIN > SWIN ? MWIN : SWIN;
 static_assert(WINMAX <= 32, "one lane per window column");
@@ -501,16 +502,24 @@ __device__ void multi_sweep(Smem& sm, double2* stage, double2* H, double2* Z, in
         ms_apply_cols(sm, buf, H, ld, kb, lo, hi, j1 + 1, j1n + 1, stage, 0, 1, lane);
         __syncwarp();
         SCHUR_STAT_T(0, 9, clock64() - cc0);
+        // window c+1 (nw <= MWIN <= 32 rows: lane = row) into shared memory,
+        // eight columns' loads in flight per lane before any is stored
         const int nw = j1n - j0n + 1;
-        for (int e = lane; e < nw * nw; e += 32) {
-          const int r = e % nw, cc = e / nw;
-          sm.Hw[cc][r] = H[(long long)(j0n + cc) * ld + j0n + r];
+        const double2* hw = H + (long long)j0n * ld + j0n + lane;
+        for (int c0 = 0; c0 < nw; c0 += 8) {
+          double2 v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            v[u] = (lane < nw && c0 + u < nw) ? hw[(long long)(c0 + u) * ld] : cmk(0.0, 0.0);
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (lane < nw && c0 + u < nw) sm.Hw[c0 + u][lane] = v[u];
         }
         __syncwarp();
         ms_chase(sm, buf ^ 1, l, i, T, (c + 1) * MW, j0n, nw, lane);
-        for (int e = lane; e < nw * nw; e += 32) {
-          const int r = e % nw, cc = e / nw;
-          H[(long long)(j0n + cc) * ld + j0n + r] = sm.Hw[cc][r];
+        if (lane < nw) {
+          double2* hwo = H + (long long)j0n * ld + j0n + lane;
+          for (int cc = 0; cc < nw; ++cc) hwo[(long long)cc * ld] = sm.Hw[cc][lane];
         }
       }
       SCHUR_STAT_T(0, 8, clock64() - cc0);
