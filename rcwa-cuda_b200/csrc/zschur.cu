@@ -282,11 +282,16 @@ __device__ void ms_chase(Smem& sm, int buf, int l, int i, int T, int t0, int j0,
 #pragma unroll 1
   for (int s = 0; s < MW; ++s) {
     const int t = t0 + s;
+    // lane b < NS computes bulge b's reflector and logs it for the far
+    // updates; the window updates below take it from lane b by shuffles
+    // (register broadcasts, all independent: no shared-memory round trip
+    // per reflector on this serial path)
+    double beta = 0.0;
+    double2 tau = cmk(0.0, 0.0), v2 = cmk(0.0, 0.0);
+    bool act = false;
     if (lane < NS) {
       const int b = lane, k = l + t - 2 * b;
-      const bool act = (t < T) && k >= l && k <= i - 1;
-      double beta = 0.0;
-      double2 tau = cmk(0.0, 0.0), v2 = cmk(0.0, 0.0);
+      act = (t < T) && k >= l && k <= i - 1;
       if (act) {
         const int kk = k - j0;
         double2 alpha, x;
@@ -304,8 +309,15 @@ __device__ void ms_chase(Smem& sm, int buf, int l, int i, int T, int t0, int j0,
       sm.rbeta[s][b] = beta;
       sm.ract[buf][s][b] = act ? 1 : 0;
     }
+    const unsigned amask = __ballot_sync(0xffffffffu, act);
     __syncwarp();
     const int base = l + t - j0 - 2 * (NS - 1);
+    double2 tb[NS], vb[NS];
+#pragma unroll
+    for (int b = 0; b < NS; ++b) {
+      tb[b] = cmk(__shfl_sync(0xffffffffu, tau.x, b), __shfl_sync(0xffffffffu, tau.y, b));
+      vb[b] = cmk(__shfl_sync(0xffffffffu, v2.x, b), __shfl_sync(0xffffffffu, v2.y, b));
+    }
     double2 x[2 * NS];
     {  // left: lane = window column c
       const int c = lane;
@@ -317,11 +329,11 @@ __device__ void ms_chase(Smem& sm, int buf, int l, int i, int T, int t0, int j0,
 #pragma unroll
       for (int b = 0; b < NS; ++b) {
         const int p = 2 * (NS - 1 - b), kk = base + p;
-        const bool act = lds1(&sm.ract[buf][s][b]) != 0;
-        const double2 tau = (act && c >= kk) ? lds2(&sm.rtau[buf][s][b]) : cmk(0.0, 0.0);
-        refl_left(x[p], x[p + 1], tau, lds2(&sm.rv[buf][s][b]));
-        if (act && c == kk - 1 && kk + j0 > l) {
-          x[p] = cmk(sm.rbeta[s][b], 0.0);
+        const bool actb = (amask >> b) & 1u;
+        const double bt = __shfl_sync(0xffffffffu, beta, b);
+        refl_left(x[p], x[p + 1], (actb && c >= kk) ? tb[b] : cmk(0.0, 0.0), vb[b]);
+        if (actb && c == kk - 1 && kk + j0 > l) {
+          x[p] = cmk(bt, 0.0);
           x[p + 1] = cmk(0.0, 0.0);
         }
       }
@@ -342,10 +354,8 @@ __device__ void ms_chase(Smem& sm, int buf, int l, int i, int T, int t0, int j0,
 #pragma unroll
       for (int b = 0; b < NS; ++b) {
         const int p = 2 * (NS - 1 - b), kk = base + p;
-        const bool act = lds1(&sm.ract[buf][s][b]) != 0;
-        const double2 tau =
-            (act && r <= min(kk + j0 + 2, i) - j0) ? lds2(&sm.rtau[buf][s][b]) : cmk(0.0, 0.0);
-        refl_right(x[p], x[p + 1], tau, lds2(&sm.rv[buf][s][b]));
+        const bool actb = (amask >> b) & 1u;
+        refl_right(x[p], x[p + 1], (actb && r <= min(kk + j0 + 2, i) - j0) ? tb[b] : cmk(0.0, 0.0), vb[b]);
       }
 #pragma unroll
       for (int q = 0; q < 2 * NS; ++q) {
