@@ -115,12 +115,6 @@ __device__ __forceinline__ double2 lds2(const double2* p) {
   asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a));
   return v;
 }
-__device__ __forceinline__ int lds1(const int* p) {
-  int v;
-  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-  asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(a));
-  return v;
-}
 
 // Eigenvalues of the m x m upper Hessenberg Hs by single-shift QR (one warp,
 // eigenvalues only).  Writes sm.shifts[0..m); false if the cap is reached.
