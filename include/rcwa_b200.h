@@ -54,10 +54,12 @@ extern "C" {
                               in reduced precision; FP64 Omega^2, eig, sqrt, exp and sums */
 
 /* Stages that RCWA_PREC_MIXED runs in reduced precision.  GEMM stages use the
- * int8-sliced tensor-core GEMM (each row of A and column of B scaled by a
- * power of two and cut into four signed 7-bit digits, digit products
+ * int8-sliced tensor-core GEMM for products with m, n, k >= 256 (each row of
+ * A and column of B scaled by a power of two and cut into signed 7-bit
+ * digits, 5 by default (4 to 6 via rcwa_context_set_mixed), digit products
  * accumulated exactly in int32 by tcgen05 kind::i8, combined in FP64: about
- * 29 bits of every product), or with RCWA_MIXED_GEMM_TF32 the split-TF32
+ * 36 bits of every product with 5 digits; smaller products stay on the FP64
+ * kernels), or with RCWA_MIXED_GEMM_TF32 the split-TF32
  * GEMM (each FP64 operand split into TF32 hi + lo, three tcgen05 kind::tf32
  * products accumulated in the tensor core's FP32).  LU stages factor and
  * solve in FP32 (complex64) and refine the solution with FP64 residuals
