@@ -49,6 +49,7 @@ constexpr int NB = 32;
 constexpr int PANEL_NT = 256;
 constexpr int PANEL_NT_WIDE = 1024;   // large n, few matrices: more rows in flight per column step
 constexpr int COL_NT = 64;
+constexpr int PCHUNK = 8;   // panel update: entries of a row in flight at once
 
 template <class T>
 struct Cx;
@@ -132,17 +133,27 @@ lu_panel_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int j, int 
     if (tid == 0 && pv.x == R(0) && pv.y == R(0)) atomicOr(status + b, (unsigned)ST_SINGULAR);
     __syncthreads();
     const T inv = crcp(pv);
-    // 4. scale the column below the pivot and rank-1 update the panel
+    // 4. scale the column below the pivot and rank-1 update the panel; the
+    // row's entries of the remaining columns are loaded PC at a time before
+    // any is stored, so their load latencies overlap (fewer at a time with
+    // 1024 threads, whose register budget is 64)
+    constexpr int PC = PNT > 256 ? 4 : PCHUNK;
     for (int r = col + 1 + tid; r < n; r += PNT) {
       T l = cmul(Mc[r], inv);
       Mc[r] = l;
-      for (int cc = c + 1; cc < jb; ++cc) {
-        T* q = M + (long long)(j + cc) * ld + r;
-        T u = s_urow[cc];
-        T v = *q;
-        v.x -= l.x * u.x - l.y * u.y;
-        v.y -= l.x * u.y + l.y * u.x;
-        *q = v;
+      for (int c0 = c + 1; c0 < jb; c0 += PC) {
+        T v[PC];
+#pragma unroll
+        for (int u = 0; u < PC; ++u)
+          if (c0 + u < jb) v[u] = M[(long long)(j + c0 + u) * ld + r];
+#pragma unroll
+        for (int u = 0; u < PC; ++u)
+          if (c0 + u < jb) {
+            const T w = s_urow[c0 + u];
+            v[u].x -= l.x * w.x - l.y * w.y;
+            v[u].y -= l.x * w.y + l.y * w.x;
+            M[(long long)(j + c0 + u) * ld + r] = v[u];
+          }
       }
     }
     __syncthreads();
@@ -491,8 +502,14 @@ int lu_factor(cudaStream_t s, int n, T* M, int ld, long long stride, int batch, 
     }
     const int cb = j + jb;
     if (cb < n) {
+      // the panel's interchanges on the trailing columns as a pass of its
+      // own (one thread per column, little register use: many columns in
+      // flight to cover the sequential swaps' latency), then L11^-1
       dim3 g(cdiv_up(n - cb, COL_NT), batch);
-      lu_swap_lsolve_kernel<T><<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, jb, cb, n, piv, 1);
+      lu_rowswap_kernel<T><<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, j + jb, cb, n, piv);
+      count_launch();
+      RCWA_LAUNCH_CHECK();
+      lu_swap_lsolve_kernel<T><<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, jb, cb, n, piv, 0);
       count_launch();
       RCWA_LAUNCH_CHECK();
       int rc = gemm_sub(s, n - cb, n - cb, jb, M + (long long)j * ld + cb, ld, stride,
