@@ -160,54 +160,97 @@ lu_panel_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int j, int 
   }
 }
 
-// Row swaps of panel j plus forward substitution with the unit-lower L11 for
-// columns [c_begin, c_end) of the augmented matrix.
+// Triangular solve with the NB x NB diagonal block at rows j..j+jb-1 for the
+// right-hand-side columns [c_begin, c_end): X = L11^-1 X (unit lower, UPPER
+// = false) or X = U11^-1 X (UPPER = true).  COL_NT columns per CTA are
+// staged through shared memory: each warp moves whole column segments with
+// one coalesced access per column (lane = row), eight columns in flight at a
+// time; then each thread solves one column in registers (the column kernels'
+// arithmetic, in the same order), and the tile goes back the same way.
+// Dynamic shared memory: trsm_smem<T>() bytes.
 template <class T>
+constexpr size_t trsm_smem() {
+  return sizeof(T) * ((size_t)(NB + COL_NT) * (NB + 1) + NB);
+}
+template <class T, bool UPPER>
 __global__ void __launch_bounds__(COL_NT)
-lu_swap_lsolve_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int j, int jb, int c_begin,
-                      int c_end, const int* __restrict__ pivg, int swap) {
+lu_trsm_tile_kernel(T* __restrict__ Mg, int ld, long long stride, int j, int jb, int c_begin, int c_end) {
+  extern __shared__ __align__(16) unsigned char tsm[];
+  T (*D)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(tsm);                                   // D[r][c]
+  T (*Xs)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(tsm + sizeof(T) * NB * (NB + 1));     // Xs[col][r]
+  T* dinv = reinterpret_cast<T*>(tsm + sizeof(T) * (NB + COL_NT) * (NB + 1));
+  constexpr int NWP = COL_NT / 32;
   const int b = blockIdx.y;
   T* M = Mg + (long long)b * stride;
-  const int* piv = pivg + (long long)b * n;
-  __shared__ T L[NB][NB + 1];  // L[r][c]
-  __shared__ int sp[NB];
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int cbase = c_begin + blockIdx.x * COL_NT;
+  const int ncol = min(COL_NT, c_end - cbase);
   for (int e = tid; e < jb * jb; e += COL_NT) {
-    int r = e % jb, c = e / jb;
-    L[r][c] = M[(long long)(j + c) * ld + j + r];
+    const int r = e % jb, c = e / jb;
+    D[r][c] = M[(long long)(j + c) * ld + j + r];
   }
-  if (swap)
-    for (int e = tid; e < jb; e += COL_NT) sp[e] = piv[j + e];
+  const T* src = M + (long long)cbase * ld + j + lane;
+  for (int c0 = wid; c0 < ncol; c0 += NWP * 8) {
+    T v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int cc = c0 + u * NWP;
+      v[u] = (cc < ncol && lane < jb) ? src[(long long)cc * ld] : Cx<T>::mk(0, 0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int cc = c0 + u * NWP;
+      if (cc < ncol && lane < jb) Xs[cc][lane] = v[u];
+    }
+  }
   __syncthreads();
-  const int col = c_begin + blockIdx.x * COL_NT + tid;
-  if (col >= c_end) return;
-  T* q = M + (long long)col * ld;
-  if (swap)
-    for (int c = 0; c < jb; ++c) {
-      int p = sp[c];
-      if (p != j + c) {
-        T t = q[j + c];
-        q[j + c] = q[p];
-        q[p] = t;
+  if (UPPER) {
+    for (int e = tid; e < jb; e += COL_NT) dinv[e] = crcp(D[e][e]);
+    __syncthreads();
+  }
+  if (tid < ncol) {
+    T x[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) x[c] = (c < jb) ? Xs[tid][c] : Cx<T>::mk(0, 0);
+    if (!UPPER) {
+#pragma unroll
+      for (int c = 0; c < NB; ++c) {
+#pragma unroll
+        for (int r = c + 1; r < NB; ++r) {
+          if (r < jb) {
+            T l = D[r][c];
+            x[r].x -= l.x * x[c].x - l.y * x[c].y;
+            x[r].y -= l.x * x[c].y + l.y * x[c].x;
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int c = NB - 1; c >= 0; --c) {
+        if (c < jb) {
+          x[c] = cmul(x[c], dinv[c]);
+#pragma unroll
+          for (int r = 0; r < c; ++r) {
+            T u = D[r][c];
+            x[r].x -= u.x * x[c].x - u.y * x[c].y;
+            x[r].y -= u.x * x[c].y + u.y * x[c].x;
+          }
+        }
       }
     }
-  T x[NB];
 #pragma unroll
-  for (int c = 0; c < NB; ++c) x[c] = (c < jb) ? q[j + c] : Cx<T>::mk(0, 0);
+    for (int c = 0; c < NB; ++c)
+      if (c < jb) Xs[tid][c] = x[c];
+  }
+  __syncthreads();
+  T* dst = M + (long long)cbase * ld + j + lane;
+  for (int c0 = wid; c0 < ncol; c0 += NWP * 8) {
 #pragma unroll
-  for (int c = 0; c < NB; ++c) {
-#pragma unroll
-    for (int r = c + 1; r < NB; ++r) {
-      if (r < jb) {
-        T l = L[r][c];
-        x[r].x -= l.x * x[c].x - l.y * x[c].y;
-        x[r].y -= l.x * x[c].y + l.y * x[c].x;
-      }
+    for (int u = 0; u < 8; ++u) {
+      const int cc = c0 + u * NWP;
+      if (cc < ncol && lane < jb) dst[(long long)cc * ld] = Xs[cc][lane];
     }
   }
-#pragma unroll
-  for (int c = 0; c < NB; ++c)
-    if (c < jb) q[j + c] = x[c];
 }
 
 // Row interchanges piv[r_begin..r_end) (in order) applied to columns
@@ -278,46 +321,6 @@ lu_gather_kernel(T* __restrict__ Mg, int ld, long long stride, int n, int c_begi
     for (int r = lane; r < n; r += 32) q[r] = sh[idx[r]];
     __syncwarp();
   }
-}
-
-// Upper-triangular solve X = U11^-1 X for rows j..j+jb-1 of the right-hand
-// side columns [c_begin, c_end).
-template <class T>
-__global__ void __launch_bounds__(COL_NT)
-lu_usolve_kernel(T* __restrict__ Mg, int ld, long long stride, int j, int jb, int c_begin, int c_end) {
-  const int b = blockIdx.y;
-  T* M = Mg + (long long)b * stride;
-  __shared__ T U[NB][NB + 1];
-  __shared__ T dinv[NB];
-  const int tid = threadIdx.x;
-  for (int e = tid; e < jb * jb; e += COL_NT) {
-    int r = e % jb, c = e / jb;
-    U[r][c] = M[(long long)(j + c) * ld + j + r];
-  }
-  __syncthreads();
-  for (int e = tid; e < jb; e += COL_NT) dinv[e] = crcp(U[e][e]);
-  __syncthreads();
-  const int col = c_begin + blockIdx.x * COL_NT + tid;
-  if (col >= c_end) return;
-  T* q = M + (long long)col * ld;
-  T x[NB];
-#pragma unroll
-  for (int c = 0; c < NB; ++c) x[c] = (c < jb) ? q[j + c] : Cx<T>::mk(0, 0);
-#pragma unroll
-  for (int c = NB - 1; c >= 0; --c) {
-    if (c < jb) {
-      x[c] = cmul(x[c], dinv[c]);
-#pragma unroll
-      for (int r = 0; r < c; ++r) {
-        T u = U[r][c];
-        x[r].x -= u.x * x[c].x - u.y * x[c].y;
-        x[r].y -= u.x * x[c].y + u.y * x[c].x;
-      }
-    }
-  }
-#pragma unroll
-  for (int c = 0; c < NB; ++c)
-    if (c < jb) q[j + c] = x[c];
 }
 
 // ---------------------------------------------------------------------------
@@ -464,6 +467,26 @@ int perm_attrs() {
   return RCWA_OK;
 }
 
+// Dynamic shared-memory limits of the triangular tile kernels (above the
+// 48 KB default for complex128), set once per device.
+int trsm_attrs() {
+  static bool set[64] = {};
+  int dev = 0;
+  RCWA_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 64 || !set[dev]) {
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(lu_trsm_tile_kernel<double2, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem<double2>()));
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(lu_trsm_tile_kernel<double2, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem<double2>()));
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(lu_trsm_tile_kernel<float2, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem<float2>()));
+    RCWA_CUDA_TRY(cudaFuncSetAttribute(lu_trsm_tile_kernel<float2, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem<float2>()));
+    if (dev < 64) set[dev] = true;
+  }
+  return RCWA_OK;
+}
+
 int panel_sms() {
   static int sms[64];
   int dev = 0;
@@ -509,7 +532,8 @@ int lu_factor(cudaStream_t s, int n, T* M, int ld, long long stride, int batch, 
       lu_rowswap_kernel<T><<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, j + jb, cb, n, piv);
       count_launch();
       RCWA_LAUNCH_CHECK();
-      lu_swap_lsolve_kernel<T><<<g, COL_NT, 0, s>>>(M, ld, stride, n, j, jb, cb, n, piv, 0);
+      if (int rc = trsm_attrs()) return rc;
+      lu_trsm_tile_kernel<T, false><<<g, COL_NT, trsm_smem<T>(), s>>>(M, ld, stride, j, jb, cb, n);
       count_launch();
       RCWA_LAUNCH_CHECK();
       int rc = gemm_sub(s, n - cb, n - cb, jb, M + (long long)j * ld + cb, ld, stride,
@@ -535,6 +559,7 @@ int lu_compose(cudaStream_t s, int n, int* piv, int batch) {
 template <class T>
 int lu_solve(cudaStream_t s, int n, int nrhs, T* M, int ld, long long stride, int batch, const int* idx) {
   if (nrhs <= 0) return RCWA_OK;
+  if (int rc = trsm_attrs()) return rc;
   const int ncols = n + nrhs;
   T* Bc = M + (long long)n * ld;   // right-hand sides, rows 0..n-1
   {
@@ -558,7 +583,7 @@ int lu_solve(cudaStream_t s, int n, int nrhs, T* M, int ld, long long stride, in
   std::function<int(int, int)> lower = [&](int r0, int r1) -> int {
     if (r1 - r0 <= NB) {
       dim3 g(cdiv_up(nrhs, COL_NT), batch);
-      lu_swap_lsolve_kernel<T><<<g, COL_NT, 0, s>>>(M, ld, stride, n, r0, r1 - r0, n, ncols, idx, 0);
+      lu_trsm_tile_kernel<T, false><<<g, COL_NT, trsm_smem<T>(), s>>>(M, ld, stride, r0, r1 - r0, n, ncols);
       count_launch();
       RCWA_LAUNCH_CHECK();
       return RCWA_OK;
@@ -574,7 +599,7 @@ int lu_solve(cudaStream_t s, int n, int nrhs, T* M, int ld, long long stride, in
   std::function<int(int, int)> upper = [&](int r0, int r1) -> int {
     if (r1 - r0 <= NB) {
       dim3 g(cdiv_up(nrhs, COL_NT), batch);
-      lu_usolve_kernel<T><<<g, COL_NT, 0, s>>>(M, ld, stride, r0, r1 - r0, n, ncols);
+      lu_trsm_tile_kernel<T, true><<<g, COL_NT, trsm_smem<T>(), s>>>(M, ld, stride, r0, r1 - r0, n, ncols);
       count_launch();
       RCWA_LAUNCH_CHECK();
       return RCWA_OK;
