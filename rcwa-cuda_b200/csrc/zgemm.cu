@@ -8,11 +8,13 @@
 // the reference's asDiagonal() products (rcwa.cpp:273-285, 329, 339) into the
 // epilogue so no dense diagonal matrix is ever materialised.
 //
-// Two FP64 kernels: the default runs on the FP64 tensor cores (DMMA, below);
-// a CUDA-core kernel (64x64 C tile, K step 8, 256 threads as 16x16, each a
-// 4x4 complex micro-tile) is kept as the alternative.  Both stage A and B
-// tiles with cp.async (16-byte copies, zero-filled outside the matrix).
-// tcgen05 has no FP64 kind, so FP64 tensor work on sm_100a is mma.sync DMMA.
+// Three FP64 kernels, chosen per shape bucket by a measured table
+// (rcwa_set_gemm_table): the FP64 tensor-core (DMMA) kernel with tiles staged
+// by cp.async (16-byte copies, zero-filled outside the matrix), the same DMMA
+// tiling fed by the tensor memory accelerator (products of operands as
+// stored), and a CUDA-core kernel (64x64 C tile, K step 8, 256 threads as
+// 16x16, each a 4x4 complex micro-tile).  tcgen05 has no FP64 kind, so FP64
+// tensor work on sm_100a is mma.sync DMMA.
 #include <atomic>
 #include <cstring>
 #include <mutex>
