@@ -389,8 +389,9 @@ int rcwa_gemm_device(rcwa_context* ctx, int m, int n, int k, int batch, rcwa_com
  * (min(m, n) <= 64, <= 128, <= 256, <= 512, larger); 0 = the FP64 tensor-core
  * (DMMA) kernel fed by cp.async, 1 = the CUDA-core kernel, 2 = the DMMA kernel
  * fed by the tensor memory accelerator (TMA; products of operands as stored,
- * others fall back to 0), -1 = the built-in rule (DMMA for k > 64).  NULL
- * restores the built-in rule.  Process-wide. */
+ * others fall back to 0), 3 = the cp.async-fed DMMA kernel with 32 x 64
+ * tiles, -1 = the built-in rule (DMMA for k > 64).  NULL restores the
+ * built-in rule.  Process-wide. */
 int rcwa_set_gemm_table(const int* choice);
 /* C = alpha op(A) op(B) + beta C, batched, column-major host arrays; op = 1
  * takes the conjugate transpose (A stored k x m, B stored n x k), C is read

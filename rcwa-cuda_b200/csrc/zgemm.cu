@@ -8,9 +8,10 @@
 // the reference's asDiagonal() products (rcwa.cpp:273-285, 329, 339) into the
 // epilogue so no dense diagonal matrix is ever materialised.
 //
-// Three FP64 kernels, chosen per shape bucket by a measured table
+// FP64 kernels chosen per shape bucket by a measured table
 // (rcwa_set_gemm_table): the FP64 tensor-core (DMMA) kernel with tiles staged
-// by cp.async (16-byte copies, zero-filled outside the matrix), the same DMMA
+// by cp.async (16-byte copies, zero-filled outside the matrix; 64 x 64 or
+// 32 x 64 complex tiles), the same DMMA
 // tiling fed by the tensor memory accelerator (products of operands as
 // stored), and a CUDA-core kernel (64x64 C tile, K step 8, 256 threads as
 // 16x16, each a 4x4 complex micro-tile).  tcgen05 has no FP64 kind, so FP64
@@ -738,11 +739,13 @@ int thin_cut(int extent) {
 
 // Kernel choice per shape bucket: k in (<=16, <=32, <=64, <=128, more) by
 // min(m, n) in (<=64, <=128, <=256, <=512, more); entry 0 = DMMA kernel fed
-// by cp.async, 1 = CUDA-core kernel, 2 = DMMA kernel fed by TMA (products
-// with both operands as stored; the others take entry 0's kernel), -1 = the
-// built-in rule (DMMA for k > 64, CUDA cores for the rank-k updates).  A
-// measured table comes from the tuner (rcwa_set_gemm_table); RCWA_ZGEMM=ffma,
-// =dmma or =tma (read once) forces one kernel for every shape.
+// by cp.async (64 x 64 tiles), 1 = CUDA-core kernel, 2 = DMMA kernel fed by
+// TMA (products with both operands as stored; the others take entry 0's
+// kernel), 3 = DMMA kernel fed by cp.async with 32 x 64 tiles (two warps),
+// -1 = the built-in rule (DMMA for k > 64, CUDA cores for the rank-k
+// updates).  A measured table comes from the tuner (rcwa_set_gemm_table);
+// RCWA_ZGEMM=ffma, =dmma, =tma or =dmma32 (read once) forces one kernel for
+// every shape.
 std::atomic<int> g_gemm_table[25];
 std::atomic<bool> g_gemm_table_init{false};
 
@@ -756,12 +759,17 @@ int gemm_impl(int m, int n, int k) {
   static int forced = -2;
   if (forced == -2) {
     const char* e = getenv("RCWA_ZGEMM");
-    forced = !e ? -1 : strcmp(e, "ffma") == 0 ? 1 : strcmp(e, "dmma") == 0 ? 0 : strcmp(e, "tma") == 0 ? 2 : -1;
+    forced = !e                           ? -1
+             : strcmp(e, "ffma") == 0     ? 1
+             : strcmp(e, "dmma") == 0     ? 0
+             : strcmp(e, "tma") == 0      ? 2
+             : strcmp(e, "dmma32") == 0   ? 3
+                                          : -1;
   }
   if (forced >= 0) return forced;
   if (g_gemm_table_init.load()) {
     const int c = g_gemm_table[gemm_bucket_k(k) * 5 + gemm_bucket_mn(m, n)].load();
-    if (c >= 0 && c <= 2) return c;
+    if (c >= 0 && c <= 3) return c;
   }
   return k > 64 ? 0 : 1;
 }
@@ -854,7 +862,7 @@ int launch_dmma(cudaStream_t s, const ZGemm& g, dim3 grid, int cm = 0, int cn = 
   const int thin_rows = cdiv_up(thin, (int)grid.x);
   grid.y = cdiv_up(mm, 32 * WM) + thin_rows;
   const int kk = g.k < 0 ? 0 : g.k;
-  if (tma && g.opA == 0 && g.opB == 0) {
+  if (WM == RCWA_DMMA_WM && tma && g.opA == 0 && g.opB == 0) {
     bool launched = false;
     const int rc = launch_dmma_tma<WM, RCWA_DMMA_TMA_ST>(s, g, grid, mm, nm, kk, thin_rows, &launched);
     if (rc || launched) return rc;
@@ -891,7 +899,9 @@ int zgemm(cudaStream_t s, const ZGemm& g) {
   g.m, g.n, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
       g.dr, g.sdr
   const int impl = gemm_impl(g.m, g.n, kk);
-  if (impl != 1) {
+  if (impl == 3) {   // 32 x 64 DMMA tiles (two warps): more CTAs for small products
+    if ((rc = launch_dmma<1, RCWA_DMMA_ST>(s, g, grid, thin_cut(g.m), thin_cut(g.n)))) return rc;
+  } else if (impl != 1) {
     if ((rc = launch_dmma<RCWA_DMMA_WM, RCWA_DMMA_ST>(s, g, grid, thin_cut(g.m), thin_cut(g.n), impl == 2)))
       return rc;
   } else {
@@ -918,8 +928,8 @@ int zgemm(cudaStream_t s, const ZGemm& g) {
 extern "C" int rcwa_set_gemm_table(const int* choice) {
   for (int i = 0; i < 25; ++i) {
     const int c = choice ? choice[i] : -1;
-    if (c < -1 || c > 2) {
-      rcwa::set_last_error("gemm table entries must be -1, 0, 1 or 2");
+    if (c < -1 || c > 3) {
+      rcwa::set_last_error("gemm table entries must be -1, 0, 1, 2 or 3");
       return RCWA_ERR_INVALID;
     }
   }

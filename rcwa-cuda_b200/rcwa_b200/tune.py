@@ -6,9 +6,10 @@ kernel table the library uses (``rcwa_set_gemm_table``).
 The solve path multiplies matrices of very different shapes: rank-32 updates
 of the blocked LU and Hessenberg reductions (k = 32), the recursive
 triangular solves (k up to n / 2) and the S-matrix algebra (k = n), for n
-from 50 to 2000.  Three FP64 kernels compete: the FP64 tensor-core (DMMA)
-kernel with cp.async tile loads, the same DMMA kernel fed by the tensor
-memory accelerator (TMA) through an mbarrier ring, and the CUDA-core kernel.  For every bucket -- k in (<= 16, <= 32,
+from 50 to 2000.  Four FP64 kernels compete: the FP64 tensor-core (DMMA)
+kernel with cp.async tile loads on 64 x 64 and on 32 x 64 complex tiles, the
+64 x 64 DMMA kernel fed by the tensor memory accelerator (TMA) through an
+mbarrier ring, and the CUDA-core kernel.  For every bucket -- k in (<= 16, <= 32,
 <= 64, <= 128, larger) by min(m, n) in (<= 64, <= 128, <= 256, <= 512,
 larger) -- the tuner times both kernels on a representative square shape,
 in both forms the solver issues (C = A B and the update C = C - A B), with a
@@ -33,7 +34,8 @@ SIZE_LIMITS = ["mn<=64", "mn<=128", "mn<=256", "mn<=512", "mn>512"]
 
 def _time_kernel(ctx, lib, torch, stream, choice, s, k, batch, reps=5):
     """Median ms of C = A B plus C = C - A B with every bucket forced to
-    `choice` (0 = DMMA with cp.async, 1 = CUDA cores, 2 = DMMA fed by TMA)."""
+    `choice` (0 = DMMA with cp.async, 1 = CUDA cores, 2 = DMMA fed by TMA,
+    3 = DMMA with cp.async on 32 x 64 tiles)."""
     import ctypes as C
     arr = (C.c_int * 25)(*([choice] * 25))
     assert lib.rcwa_set_gemm_table(arr) == 0
@@ -68,21 +70,22 @@ def tune(path: str = TABLE_PATH) -> dict:
             for s in SIZE_BUCKETS:
                 flops = 2 * 8.0 * s * s * k
                 batch = int(max(1, min(4096, 4e9 / flops)))
-                t = [_time_kernel(ctx, lib, torch, stream, c, s, k, batch) for c in (0, 1, 2)]
-                choice = min(range(3), key=lambda c: t[c])
+                t = [_time_kernel(ctx, lib, torch, stream, c, s, k, batch) for c in (0, 1, 2, 3)]
+                choice = min(range(4), key=lambda c: t[c])
                 table.append(choice)
                 rows.append({"k": k, "m=n": s, "batch": batch,
                              "dmma_tflops": flops * batch / (t[0] / 1e3) / 1e12,
                              "cuda_core_tflops": flops * batch / (t[1] / 1e3) / 1e12,
                              "dmma_tma_tflops": flops * batch / (t[2] / 1e3) / 1e12,
-                             "choice": ("dmma", "cuda_core", "dmma_tma")[choice]})
+                             "dmma_32x64_tflops": flops * batch / (t[3] / 1e3) / 1e12,
+                             "choice": ("dmma", "cuda_core", "dmma_tma", "dmma_32x64")[choice]})
     finally:
         lib.rcwa_set_gemm_table(None)
         ctx.close()
     out = {"device": torch.cuda.get_device_name(0), "date": time.strftime("%Y-%m-%d"),
            "k_buckets": K_LIMITS, "size_buckets": SIZE_LIMITS,
            "choice": table, "measurements": rows,
-           "note": "choice[5 * k_bucket + size_bucket]: 0 = FP64 tensor-core (DMMA) kernel fed by cp.async, 1 = CUDA-core kernel, 2 = DMMA kernel fed by TMA"}
+           "note": "choice[5 * k_bucket + size_bucket]: 0 = FP64 tensor-core (DMMA) kernel fed by cp.async, 1 = CUDA-core kernel, 2 = DMMA kernel fed by TMA, 3 = DMMA kernel (cp.async) on 32 x 64 tiles"}
     with open(path, "w") as f:
         json.dump(out, f, indent=1)
     return out
@@ -95,7 +98,7 @@ def load_table(path: str = TABLE_PATH):
     with open(path) as f:
         t = json.load(f)
     ch = t.get("choice")
-    if not isinstance(ch, list) or len(ch) != 25 or any(c not in (-1, 0, 1, 2) for c in ch):
+    if not isinstance(ch, list) or len(ch) != 25 or any(c not in (-1, 0, 1, 2, 3) for c in ch):
         return None
     return ch
 

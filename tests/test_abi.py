@@ -67,20 +67,21 @@ def test_cpp_host_api_compiles_and_links(lib, tmp_path):
 
 
 def test_gemm_table_choices_without_gpu(lib, tmp_path):
-    """Kernel-table entries 0, 1, 2 (DMMA via cp.async, CUDA cores, DMMA via
-    TMA) and -1 are accepted, anything else is rejected; the tuner's table
-    loader applies the same rule."""
+    """Kernel-table entries 0, 1, 2, 3 (DMMA via cp.async, CUDA cores, DMMA
+    via TMA, DMMA via cp.async on 32 x 64 tiles) and -1 are accepted,
+    anything else is rejected; the tuner's table loader applies the same
+    rule."""
     import json
     from rcwa_b200 import lib as L
     from rcwa_b200 import tune
-    ok = (ctypes.c_int * 25)(*([2] * 12 + [0] * 6 + [1] * 6 + [-1]))
+    ok = (ctypes.c_int * 25)(*([2] * 12 + [0] * 6 + [1] * 3 + [3] * 3 + [-1]))
     assert lib.rcwa_set_gemm_table(ok) == L.RCWA_OK
-    bad = (ctypes.c_int * 25)(*([0] * 24 + [3]))
+    bad = (ctypes.c_int * 25)(*([0] * 24 + [4]))
     assert lib.rcwa_set_gemm_table(bad) == L.RCWA_ERR_INVALID
     assert lib.rcwa_set_gemm_table(None) == L.RCWA_OK
     p = tmp_path / "t.json"
     p.write_text(json.dumps({"choice": [2] * 25}))
     assert tune.load_table(str(p)) == [2] * 25
-    p.write_text(json.dumps({"choice": [3] * 25}))
+    p.write_text(json.dumps({"choice": [4] * 25}))
     assert tune.load_table(str(p)) is None
     assert tune.load_table(tune.TABLE_PATH) is not None

@@ -1,7 +1,8 @@
-"""The three FP64 GEMM kernels behind every complex product, each forced
-for every shape through the kernel table (rcwa_set_gemm_table): the DMMA
-kernel fed by cp.async (0), the CUDA-core kernel (1) and the DMMA kernel
-fed by the tensor memory accelerator (2).  Each is checked against numpy on
+"""The FP64 GEMM kernels behind every complex product, each forced for every
+shape through the kernel table (rcwa_set_gemm_table): the DMMA kernel fed
+by cp.async (0), the CUDA-core kernel (1), the DMMA kernel fed by the
+tensor memory accelerator (2) and the cp.async-fed DMMA kernel on 32 x 64
+tiles (3).  Each is checked against numpy on
 the product form (alpha A B + beta C) and on the LU / Hessenberg update form
 (C - A B), at shapes with ragged edges, thin strips and rank-32 updates, and
 the TMA-fed kernel runs a whole solve against the FP64 oracle.  Tolerance as
@@ -49,7 +50,7 @@ def _rand(rng, *shape):
     return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
 
 
-@pytest.mark.parametrize("choice", [0, 1, 2])
+@pytest.mark.parametrize("choice", [0, 1, 2, 3])
 @pytest.mark.parametrize("m,n,k,b", SHAPES)
 def test_product_and_update_forms(ctx, force, choice, m, n, k, b):
     force(choice)
