@@ -70,11 +70,10 @@ __device__ unsigned long long g_schur_stats[16];
 struct Smem {
   double2 Hw[WINMAX][WINMAX + 1];  // window, Hw[col][row]
   // multishift reflector log of a chunk, double buffered (chase of chunk c+1
-  // runs while chunk c is applied): tau, v2, active flag
+  // runs while chunk c is applied): tau, v2 (inactive reflectors logged as
+  // zeros, the identity)
   double2 rtau[2][MW][NS];
   double2 rv[2][MW][NS];
-  int ract[2][MW][NS];
-  double rbeta[MW][NS];
   double2 stau[SW];
   double2 sv[SW];
   double2 Hs[NS][NS + 1];          // trailing block for the shifts, Hs[col][row]
@@ -300,8 +299,6 @@ __device__ void ms_chase(Smem& sm, int buf, int l, int i, int T, int t0, int j0,
       }
       sm.rtau[buf][s][b] = tau;
       sm.rv[buf][s][b] = v2;
-      sm.rbeta[s][b] = beta;
-      sm.ract[buf][s][b] = act ? 1 : 0;
     }
     const unsigned amask = __ballot_sync(0xffffffffu, act);
     __syncwarp();
