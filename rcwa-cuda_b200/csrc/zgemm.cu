@@ -862,10 +862,12 @@ int launch_dmma(cudaStream_t s, const ZGemm& g, dim3 grid, int cm = 0, int cn = 
   const int thin_rows = cdiv_up(thin, (int)grid.x);
   grid.y = cdiv_up(mm, 32 * WM) + thin_rows;
   const int kk = g.k < 0 ? 0 : g.k;
-  if (WM == RCWA_DMMA_WM && tma && g.opA == 0 && g.opB == 0) {
-    bool launched = false;
-    const int rc = launch_dmma_tma<WM, RCWA_DMMA_TMA_ST>(s, g, grid, mm, nm, kk, thin_rows, &launched);
-    if (rc || launched) return rc;
+  if constexpr (WM == RCWA_DMMA_WM) {   // the TMA feed exists for the default tile only
+    if (tma && g.opA == 0 && g.opB == 0) {
+      bool launched = false;
+      const int rc = launch_dmma_tma<WM, RCWA_DMMA_TMA_ST>(s, g, grid, mm, nm, kk, thin_rows, &launched);
+      if (rc || launched) return rc;
+    }
   }
 #define RCWA_DMMA_ARGS                                                                           \
   mm, nm, kk, g.alpha, g.A, g.lda, g.sA, g.B, g.ldb, g.sB, g.beta, g.C, g.ldc, g.sC, g.dl, g.sdl, \
